@@ -1,0 +1,636 @@
+// gtap_programs.cuh -- the built-in task functions, hand-lowered into the
+// switch-statement state machine that clang-gtap emits for
+// `#pragma gtap task` / `taskwait` / `queue(expr)` (the compiler itself is an
+// empty submodule in the reference, so the lowering is written out here).
+//
+// Each task follows the reference's task body (paths relative to the
+// reference project root); the cited lines are the algorithm being lowered.
+// Two lowering choices differ from the reference's generated code but not its
+// results:
+//   * a child writes its return value straight into the parent's frame (the
+//     byte offset travels in the child frame) instead of the parent reading a
+//     retained child frame after the join;
+//   * tasks that never taskwait (n-queens, BFS) spawn "detached" children,
+//     which is what GTAP_ASSUME_NO_TASKWAIT builds do in the reference.
+#pragma once
+#include "gtap_thread_sched.cuh"
+
+namespace gtap {
+namespace prog {
+
+enum : int { K_FIB = 1, K_NQ = 2, K_CILKSORT = 3, K_CILKMERGE = 4, K_MERGESORT = 5, K_BFS = 6, K_TREESUM = 7 };
+
+constexpr int kFrameBytes = 32;
+
+// ---------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ const gtap_root& root_of(const Arena& A, const WarpShared& S) {
+    return A.roots[S.l_root[lane_id()]];
+}
+
+// Return an int value: into the parent's frame at byte offset `slot`, or into
+// the root result for a root task.
+__device__ __forceinline__ void return_i32(const Arena& A, const WarpShared& S, int slot, int value) {
+    const int parent = S.l_parent[lane_id()];
+    if (parent >= 0) {
+        *reinterpret_cast<int*>(reinterpret_cast<char*>(frame_of(A, parent)) + slot) = value;
+    } else {
+        A.results[S.l_root[lane_id()]].value = value;
+    }
+}
+__device__ __forceinline__ void return_i64(const Arena& A, const WarpShared& S, int slot, long long value) {
+    const int parent = S.l_parent[lane_id()];
+    if (parent >= 0) {
+        *reinterpret_cast<long long*>(reinterpret_cast<char*>(frame_of(A, parent)) + slot) = value;
+    } else {
+        A.results[S.l_root[lane_id()]].value = value;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// fib -- evaluation/2-comparison/fib/gtap_fib.cu:10-22 (cutoff 0) and
+// evaluation/3-epaq/fib/fib_queue_1.cu:9-26 (n < cutoff runs fib_sequential);
+// EPAQ variant fib_queue_3.cu:16-26 when root.i2 != 0 and Q >= 3.
+// ---------------------------------------------------------------------------
+struct FibFrame {
+    int n;
+    int a;     // result of fib(n-1), written by child 1
+    int b;     // result of fib(n-2), written by child 2
+    int slot;  // byte offset of this task's result in its parent's frame
+};
+
+__device__ __noinline__ int fib_sequential(int n) {
+    // fib_queue_1.cu:9-14: the same doubly recursive work the reference does
+    if (n < 2) return n;
+    return fib_sequential(n - 1) + fib_sequential(n - 2);
+}
+
+__device__ __forceinline__ void fib_task(const Arena& A, WarpShared& S, void* frame, const int4& w0) {
+    FibFrame* f = reinterpret_cast<FibFrame*>(frame);
+    int4 fr = w0;   // {n, a, b, slot}, loaded with the header
+    switch (rt_state(S)) {
+        case 0: {
+            const gtap_root& rd = root_of(A, S);
+            const int n = fr.x, cutoff = rd.i1;
+            if (n < 2) {
+                return_i32(A, S, fr.w, n);
+                rt_finish(S);
+                return;
+            }
+            if (n < cutoff) {
+                return_i32(A, S, fr.w, fib_sequential(n));
+                rt_finish(S);
+                return;
+            }
+            const bool epaq = rd.i2 != 0 && A.num_queues >= 3;
+            int cc = 0;
+            FibFrame* c1 = reinterpret_cast<FibFrame*>(
+                rt_spawn(A, S, K_FIB, epaq ? ((n - 1) < cutoff ? 1 : 0) : 0, &cc, nullptr, false, false));
+            *reinterpret_cast<int4*>(c1) = make_int4(n - 1, 0, 0, 4);
+            FibFrame* c2 = reinterpret_cast<FibFrame*>(
+                rt_spawn(A, S, K_FIB, epaq ? ((n - 2) < cutoff ? 1 : 0) : 0, &cc, nullptr, false, false));
+            *reinterpret_cast<int4*>(c2) = make_int4(n - 2, 0, 0, 8);
+            if (rt_join(A, S, cc, 1, epaq ? 2 : 0)) return;
+            fr = ld_cg_v4(f);
+        }
+        // fallthrough
+        case 1: {
+            return_i32(A, S, fr.w, fr.y + fr.z);
+            rt_finish(S);
+            return;
+        }
+        default:
+            GTAP_ERROR(A, ERR_INVALID_TASKWAIT, S.l_tid[lane_id()], -1, rt_state(S), 1);
+            rt_finish(S);
+            return;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// n-queens -- evaluation/2-comparison/nq/gtap_nq.cu:10-55 (no-taskwait build)
+// ---------------------------------------------------------------------------
+struct NqFrame {
+    int meta;          // row | n << 8 | cutoff_depth << 16
+    unsigned column;
+    unsigned left;
+    unsigned right;
+};
+
+__device__ __noinline__ int nq_serial(int row, unsigned column, unsigned left, unsigned right, int n) {
+    // gtap_nq.cu:10-23 serial_search, returning the count instead of atomics
+    if (row == n) return 1;
+    const unsigned mask = (n < 32 ? (1u << n) - 1u : 0xFFFFFFFFu);
+    unsigned avail = mask & ~(column | left | right);
+    int total = 0;
+    while (avail) {
+        unsigned p = avail & (0u - avail);
+        avail -= p;
+        total += nq_serial(row + 1, column | p, (left | p) << 1, (right | p) >> 1, n);
+    }
+    return total;
+}
+
+__device__ __forceinline__ void nq_task(const Arena& A, WarpShared& S, void* frame, const int4& w0) {
+    (void)frame;
+    const int4 fr = w0;
+    const int row = fr.x & 0xFF, n = (fr.x >> 8) & 0xFF, cutoff = (fr.x >> 16) & 0xFF;
+    const unsigned column = (unsigned)fr.y, left = (unsigned)fr.z, right = (unsigned)fr.w;
+    if (row > cutoff) {
+        S.l_value[lane_id()] += nq_serial(row, column, left, right, n);
+        rt_finish(S);
+        return;
+    }
+    const unsigned mask = (n < 32 ? (1u << n) - 1u : 0xFFFFFFFFu);
+    unsigned avail = mask & ~(column | left | right);
+    while (avail) {
+        unsigned p = avail & (0u - avail);
+        avail -= p;
+        NqFrame* c = reinterpret_cast<NqFrame*>(rt_spawn(A, S, K_NQ, 0, nullptr, nullptr, false, true));
+        *reinterpret_cast<int4*>(c) =
+            make_int4(fr.x + 1, (int)(column | p), (int)((left | p) << 1), (int)((right | p) >> 1));
+    }
+    rt_finish(S);
+}
+
+// ---------------------------------------------------------------------------
+// cilksort / cilkmerge -- examples/cilksort/cilksort.cu:17-164
+// ---------------------------------------------------------------------------
+struct SortFrame {
+    int* arr;          // sorted in place (cilksort.cu `arr`)
+    int* tmp;          // scratch (cilksort.cu `tmp`)
+    const int* src;    // unsorted input read by the leaves (so repeated runs need no restore)
+    int n;
+    int pad;
+};
+struct MergeFrame {
+    const int* a;
+    const int* b;
+    int* dst;
+    int alen;
+    int blen;
+};
+static_assert(sizeof(SortFrame) <= kFrameBytes && sizeof(MergeFrame) <= kFrameBytes, "frame size");
+
+// cilksort.cu:51-86: 64-element bitonic network in registers, padded with INT_MAX
+__device__ __noinline__ void sort_small(const int* in, int* out, int n) {
+    int buf[64];
+#pragma unroll
+    for (int i = 0; i < 64; ++i) buf[i] = (i < n) ? ld_cg(in + i) : 0x7fffffff;
+#pragma unroll
+    for (int k = 2; k <= 64; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+#pragma unroll
+            for (int i = 0; i < 64; ++i) {
+                const int ixj = i ^ j;
+                if (ixj > i) {
+                    const bool up = ((i & k) == 0);
+                    const int a = buf[i], b = buf[ixj];
+                    const bool swap = up ? (a > b) : (a < b);
+                    buf[i] = swap ? b : a;
+                    buf[ixj] = swap ? a : b;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 64; ++i)
+        if (i < n) out[i] = buf[i];
+}
+
+// cilksort.cu:17-36
+__device__ __noinline__ void merge_seq(const int* a, int alen, const int* b, int blen, int* dst) {
+    int i = 0, j = 0, k = 0;
+    int av = (alen > 0) ? ld_cg(a) : 0, bv = (blen > 0) ? ld_cg(b) : 0;
+    while (i < alen && j < blen) {
+        if (av < bv) {
+            dst[k++] = av;
+            if (++i < alen) av = ld_cg(a + i);
+        } else {
+            dst[k++] = bv;
+            if (++j < blen) bv = ld_cg(b + j);
+        }
+    }
+    while (i < alen) dst[k++] = ld_cg(a + i++);
+    while (j < blen) dst[k++] = ld_cg(b + j++);
+}
+
+// cilksort.cu:38-49: largest index with x[idx] <= val
+__device__ __forceinline__ int bsearch_le(const int* x, int len, int val) {
+    int low = -1, high = len;
+    while (low + 1 < high) {
+        int mid = (low + high) / 2;
+        if (ld_cg(x + mid) <= val) low = mid;
+        else high = mid;
+    }
+    return low;
+}
+
+__device__ __forceinline__ void spawn_merge(const Arena& A, WarpShared& S, int* cc, const int* a, int alen,
+                                            const int* b, int blen, int* dst) {
+    MergeFrame* m = reinterpret_cast<MergeFrame*>(rt_spawn(A, S, K_CILKMERGE, 0, cc, nullptr, false, false));
+    m->a = a;
+    m->b = b;
+    m->dst = dst;
+    m->alen = alen;
+    m->blen = blen;
+}
+
+// cilksort.cu:89-125
+__device__ __forceinline__ void cilkmerge_task(const Arena& A, WarpShared& S, void* frame, const int4& w0,
+                                               const int4& w1) {
+    if (rt_state(S) != 0) {  // resumed after the taskwait: nothing left to do
+        rt_finish(S);
+        return;
+    }
+    const MergeFrame* f = reinterpret_cast<const MergeFrame*>(frame);
+    const int* a = reinterpret_cast<const int*>((unsigned long long)(unsigned)w0.x | ((unsigned long long)(unsigned)w0.y << 32));
+    const int* b = reinterpret_cast<const int*>((unsigned long long)(unsigned)w0.z | ((unsigned long long)(unsigned)w0.w << 32));
+    int* dst = reinterpret_cast<int*>((unsigned long long)(unsigned)w1.x | ((unsigned long long)(unsigned)w1.y << 32));
+    int alen = w1.z, blen = w1.w;
+    (void)f;
+    if (alen < blen) {
+        const int* t = a; a = b; b = t;
+        int tl = alen; alen = blen; blen = tl;
+    }
+    if (blen == 0) {
+        for (int i = 0; i < alen; ++i) dst[i] = ld_cg(a + i);
+        rt_finish(S);
+        return;
+    }
+    const int cutoff = root_of(A, S).i1;
+    if (alen + blen < cutoff) {
+        merge_seq(a, alen, b, blen, dst);
+        rt_finish(S);
+        return;
+    }
+    const int as = (alen + 1) / 2;
+    const int bs = bsearch_le(b, blen, ld_cg(a + as - 1)) + 1;
+    int cc = 0;
+    spawn_merge(A, S, &cc, a, as, b, bs, dst);
+    spawn_merge(A, S, &cc, a + as, alen - as, b + bs, blen - bs, dst + as + bs);
+    if (rt_join(A, S, cc, 1, 0)) return;
+    rt_finish(S);
+}
+
+__device__ __forceinline__ void spawn_sort(const Arena& A, WarpShared& S, int* cc, int* arr, int* tmp,
+                                           const int* src, int n) {
+    SortFrame* c = reinterpret_cast<SortFrame*>(rt_spawn(A, S, K_CILKSORT, 0, cc, nullptr, false, false));
+    c->arr = arr;
+    c->tmp = tmp;
+    c->src = src;
+    c->n = n;
+}
+
+// cilksort.cu:127-164
+__device__ __forceinline__ void cilksort_task(const Arena& A, WarpShared& S, void* frame, const int4& w0,
+                                              const int4& w1) {
+    (void)frame;
+    int* arr = reinterpret_cast<int*>((unsigned long long)(unsigned)w0.x | ((unsigned long long)(unsigned)w0.y << 32));
+    int* tmp = reinterpret_cast<int*>((unsigned long long)(unsigned)w0.z | ((unsigned long long)(unsigned)w0.w << 32));
+    const int* src = reinterpret_cast<const int*>((unsigned long long)(unsigned)w1.x | ((unsigned long long)(unsigned)w1.y << 32));
+    const int n = w1.z;
+    const int len12 = n / 2, len1 = len12 / 2, len2 = len12 - len1;
+    const int len34 = n - len12, len3 = len34 / 2, len4 = len34 - len3;
+    int cc = 0;
+    switch (rt_state(S)) {
+        case 0: {
+            const int sort_cutoff = root_of(A, S).i0;
+            if (n < sort_cutoff) {
+                sort_small(src, arr, n);
+                rt_finish(S);
+                return;
+            }
+            spawn_sort(A, S, &cc, arr, tmp, src, len1);
+            spawn_sort(A, S, &cc, arr + len1, tmp + len1, src + len1, len2);
+            spawn_sort(A, S, &cc, arr + len12, tmp + len12, src + len12, len3);
+            spawn_sort(A, S, &cc, arr + len12 + len3, tmp + len12 + len3, src + len12 + len3, len4);
+            if (rt_join(A, S, cc, 1, 0)) return;
+        }
+        // fallthrough
+        case 1: {
+            cc = 0;
+            spawn_merge(A, S, &cc, arr, len1, arr + len1, len2, tmp);
+            spawn_merge(A, S, &cc, arr + len12, len3, arr + len12 + len3, len4, tmp + len12);
+            if (rt_join(A, S, cc, 2, 0)) return;
+        }
+        // fallthrough
+        case 2: {
+            cc = 0;
+            spawn_merge(A, S, &cc, tmp, len12, tmp + len12, len34, arr);
+            if (rt_join(A, S, cc, 3, 0)) return;
+        }
+        // fallthrough
+        case 3:
+            rt_finish(S);
+            return;
+        default:
+            GTAP_ERROR(A, ERR_INVALID_TASKWAIT, S.l_tid[lane_id()], -1, rt_state(S), 3);
+            rt_finish(S);
+            return;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// mergesort -- examples/mergesort/mergesort.cu:34-50 recursion (n > cutoff
+// forks the two halves [left, mid] / [mid+1, right]); the merge after the
+// taskwait is the parallel cilkmerge above, with ping-pong buffers instead of
+// merge_device's single-thread merge and copy-back.
+// ---------------------------------------------------------------------------
+struct MsFrame {
+    const int* in;   // unsorted input
+    int* out;        // sorted output
+    int* tmp;        // scratch of the same size
+    int n;
+    int pad;
+};
+static_assert(sizeof(MsFrame) <= kFrameBytes, "frame size");
+
+// leaf: <= 64 keys through the register network, <= 128 as two halves + merge
+__device__ __noinline__ void leaf_sort(const int* in, int* out, int* scratch, int n) {
+    if (n <= 64) {
+        sort_small(in, out, n);
+        return;
+    }
+    sort_small(in, scratch, 64);
+    sort_small(in + 64, scratch + 64, n - 64);
+    merge_seq(scratch, 64, scratch + 64, n - 64, out);
+}
+
+__device__ __forceinline__ void mergesort_task(const Arena& A, WarpShared& S, void* frame, const int4& w0,
+                                               const int4& w1) {
+    (void)frame;
+    const int* in = reinterpret_cast<const int*>((unsigned long long)(unsigned)w0.x | ((unsigned long long)(unsigned)w0.y << 32));
+    int* out = reinterpret_cast<int*>((unsigned long long)(unsigned)w0.z | ((unsigned long long)(unsigned)w0.w << 32));
+    int* tmp = reinterpret_cast<int*>((unsigned long long)(unsigned)w1.x | ((unsigned long long)(unsigned)w1.y << 32));
+    const int n = w1.z;
+    const int nl = (n + 1) / 2;   // [left, mid] holds ceil(n/2) keys
+    int cc = 0;
+    switch (rt_state(S)) {
+        case 0: {
+            const int cutoff = root_of(A, S).i0;
+            if (n <= cutoff || n <= 1) {
+                if (n > 0) leaf_sort(in, out, tmp, n);
+                rt_finish(S);
+                return;
+            }
+            // children sort into tmp, using out as their scratch
+            MsFrame* c1 = reinterpret_cast<MsFrame*>(rt_spawn(A, S, K_MERGESORT, 0, &cc, nullptr, false, false));
+            c1->in = in;
+            c1->out = tmp;
+            c1->tmp = out;
+            c1->n = nl;
+            MsFrame* c2 = reinterpret_cast<MsFrame*>(rt_spawn(A, S, K_MERGESORT, 0, &cc, nullptr, false, false));
+            c2->in = in + nl;
+            c2->out = tmp + nl;
+            c2->tmp = out + nl;
+            c2->n = n - nl;
+            if (rt_join(A, S, cc, 1, 0)) return;
+        }
+        // fallthrough
+        case 1: {
+            cc = 0;
+            spawn_merge(A, S, &cc, tmp, nl, tmp + nl, n - nl, out);
+            if (rt_join(A, S, cc, 2, 0)) return;
+        }
+        // fallthrough
+        case 2:
+            rt_finish(S);
+            return;
+        default:
+            GTAP_ERROR(A, ERR_INVALID_TASKWAIT, S.l_tid[lane_id()], -1, rt_state(S), 2);
+            rt_finish(S);
+            return;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// asynchronous BFS -- examples/asynchronous_bfs/asynchronous_bfs_thread.cu:19-49
+// (atomicMin relaxation, spawn per improved vertex).  A vertex whose edge
+// range exceeds the split threshold is halved recursively, so a task never
+// spawns more than max(2, threshold) children.
+// ---------------------------------------------------------------------------
+struct BfsFrame {
+    int v;
+    int start;   // -1: whole adjacency of v
+    int end;
+    int pad;
+};
+
+__device__ __forceinline__ void bfs_task(const Arena& A, WarpShared& S, void* frame, const int4& w0) {
+    (void)frame;
+    const int4 fr = w0;
+    const gtap_root& rd = root_of(A, S);
+    const int* row = reinterpret_cast<const int*>(rd.p0);
+    const int* col = reinterpret_cast<const int*>(rd.p1);
+    int* depth = reinterpret_cast<int*>(rd.p2);
+    const int split = rd.i1 > 0 ? rd.i1 : 32;
+    const int v = fr.x;
+    int start = fr.y, end = fr.z;
+    if (start < 0) {
+        start = __ldg(row + v);
+        end = __ldg(row + v + 1);
+    }
+    if (end - start > split) {
+        const int mid = start + (end - start) / 2;
+        BfsFrame* c1 = reinterpret_cast<BfsFrame*>(rt_spawn(A, S, K_BFS, 0, nullptr, nullptr, false, true));
+        *reinterpret_cast<int4*>(c1) = make_int4(v, start, mid, 0);
+        BfsFrame* c2 = reinterpret_cast<BfsFrame*>(rt_spawn(A, S, K_BFS, 0, nullptr, nullptr, false, true));
+        *reinterpret_cast<int4*>(c2) = make_int4(v, mid, end, 0);
+        rt_finish(S);
+        return;
+    }
+    const int dv = ld_cg(depth + v);
+    for (int e = start; e < end; ++e) {
+        const int u = __ldg(col + e);
+        const int nd = dv + 1;
+        const int old = atomicMin(depth + u, nd);
+        if (old > nd) {
+            BfsFrame* c = reinterpret_cast<BfsFrame*>(rt_spawn(A, S, K_BFS, 0, nullptr, nullptr, false, true));
+            *reinterpret_cast<int4*>(c) = make_int4(u, -1, -1, 0);
+        }
+    }
+    rt_finish(S);
+}
+
+// ---------------------------------------------------------------------------
+// tree sum over a pointer-linked binary tree (new served workload; the shape
+// follows the reference's tree programs, examples/binary_tree/binary_tree_thread.cu:63-114,
+// with int32 payloads summed into int64).
+// ---------------------------------------------------------------------------
+struct TreeFrame {
+    int node;
+    int slot;         // byte offset of this task's sum in its parent's frame
+    long long a;      // left subtree sum
+    long long b;      // right subtree sum
+};
+static_assert(sizeof(TreeFrame) <= kFrameBytes, "frame size");
+
+__device__ __noinline__ long long tree_serial(const int* left, const int* right, const int* value, int node) {
+    int stack[64];
+    int sp = 0;
+    long long total = 0;
+    stack[sp++] = node;
+    while (sp > 0) {
+        const int v = stack[--sp];
+        total += __ldg(value + v);
+        const int l = __ldg(left + v), r = __ldg(right + v);
+        if (r >= 0) {
+            if (sp < 64) stack[sp++] = r;
+            else total += tree_serial(left, right, value, r);
+        }
+        if (l >= 0) {
+            if (sp < 64) stack[sp++] = l;
+            else total += tree_serial(left, right, value, l);
+        }
+    }
+    return total;
+}
+
+__device__ __forceinline__ void treesum_task(const Arena& A, WarpShared& S, void* frame, const int4& pw0,
+                                             const int4& pw1) {
+    TreeFrame* f = reinterpret_cast<TreeFrame*>(frame);
+    const gtap_root& rd = root_of(A, S);
+    const int* left = reinterpret_cast<const int*>(rd.p0);
+    const int* right = reinterpret_cast<const int*>(rd.p1);
+    const int* value = reinterpret_cast<const int*>(rd.p2);
+    const int* size = reinterpret_cast<const int*>(rd.p3);
+    int4 w0 = pw0, w1 = pw1;
+    const int node = w0.x, slot = w0.y;
+    switch (rt_state(S)) {
+        case 0: {
+            if (__ldg(size + node) <= rd.i1) {
+                return_i64(A, S, slot, tree_serial(left, right, value, node));
+                rt_finish(S);
+                return;
+            }
+            f->a = 0;
+            f->b = 0;
+            int cc = 0;
+            const int l = __ldg(left + node), r = __ldg(right + node);
+            if (l >= 0) {
+                TreeFrame* c = reinterpret_cast<TreeFrame*>(rt_spawn(A, S, K_TREESUM, 0, &cc, nullptr, false, false));
+                *reinterpret_cast<int4*>(c) = make_int4(l, 8, 0, 0);
+            }
+            if (r >= 0) {
+                TreeFrame* c = reinterpret_cast<TreeFrame*>(rt_spawn(A, S, K_TREESUM, 0, &cc, nullptr, false, false));
+                *reinterpret_cast<int4*>(c) = make_int4(r, 16, 0, 0);
+            }
+            if (rt_join(A, S, cc, 1, 0)) return;
+            w0 = ld_cg_v4(frame);   // no child spawned: a, b are the zeros stored above
+            w1 = ld_cg_v4(reinterpret_cast<const char*>(frame) + 16);
+        }
+        // fallthrough
+        case 1: {
+            const long long a = (long long)(((unsigned long long)(unsigned)w0.w << 32) | (unsigned)w0.z);
+            const long long b = (long long)(((unsigned long long)(unsigned)w1.y << 32) | (unsigned)w1.x);
+            return_i64(A, S, slot, (long long)__ldg(value + node) + a + b);
+            rt_finish(S);
+            return;
+        }
+        default:
+            GTAP_ERROR(A, ERR_INVALID_TASKWAIT, S.l_tid[lane_id()], -1, rt_state(S), 1);
+            rt_finish(S);
+            return;
+    }
+}
+
+}  // namespace prog
+
+// ---------------------------------------------------------------------------
+// Program: dispatch by kind (a switch, not an indirect call)
+// ---------------------------------------------------------------------------
+// kSorts = false leaves the register-heavy sorting kinds out of the kernel,
+// which lets fib / n-queens / BFS / tree launches run at higher occupancy.
+template <bool kSorts>
+struct BuiltinProgramT {
+    static constexpr int kFrameBytes = prog::kFrameBytes;
+
+    __device__ static int root_kind(int k) {
+        switch (k) {
+            case GTAP_KIND_FIB: return prog::K_FIB;
+            case GTAP_KIND_NQ: return prog::K_NQ;
+            case GTAP_KIND_CILKSORT: return prog::K_CILKSORT;
+            case GTAP_KIND_MERGESORT: return prog::K_MERGESORT;
+            case GTAP_KIND_BFS: return prog::K_BFS;
+            case GTAP_KIND_TREESUM: return prog::K_TREESUM;
+            default: return -1;
+        }
+    }
+
+    __device__ static void init_root(const Arena& A, const gtap_root& rd, void* frame) {
+        (void)A;
+        int4* f = reinterpret_cast<int4*>(frame);
+        switch (rd.kind) {
+            case GTAP_KIND_FIB:
+                f[0] = make_int4(rd.i0, 0, 0, 0);
+                break;
+            case GTAP_KIND_NQ:
+                f[0] = make_int4(0 | (rd.i0 << 8) | (rd.i1 << 16), 0, 0, 0);
+                break;
+            case GTAP_KIND_CILKSORT: {
+                prog::SortFrame* s = reinterpret_cast<prog::SortFrame*>(frame);
+                s->arr = reinterpret_cast<int*>(rd.p1);
+                s->tmp = reinterpret_cast<int*>(rd.p2);
+                s->src = reinterpret_cast<const int*>(rd.p0);
+                s->n = (int)rd.n;
+                break;
+            }
+            case GTAP_KIND_MERGESORT: {
+                prog::MsFrame* s = reinterpret_cast<prog::MsFrame*>(frame);
+                s->in = reinterpret_cast<const int*>(rd.p0);
+                s->out = reinterpret_cast<int*>(rd.p1);
+                s->tmp = reinterpret_cast<int*>(rd.p2);
+                s->n = (int)rd.n;
+                break;
+            }
+            case GTAP_KIND_BFS: {
+                // asynchronous_bfs_thread.cu:51-55: depth[source] = 0 before the entry task
+                int* depth = reinterpret_cast<int*>(rd.p2);
+                depth[rd.i0] = 0;
+                f[0] = make_int4(rd.i0, -1, -1, 0);
+                break;
+            }
+            case GTAP_KIND_TREESUM:
+                f[0] = make_int4(rd.i0, 0, 0, 0);
+                f[1] = make_int4(0, 0, 0, 0);
+                break;
+            default:
+                break;
+        }
+    }
+
+    // w0/w1: the first 32 frame bytes, loaded together with the header
+    __device__ static void exec(const Arena& A, WarpShared& S, int kind, int tid, void* frame, const int4& w0,
+                                const int4& w1) {
+        (void)tid;
+        switch (kind) {
+            case prog::K_FIB: prog::fib_task(A, S, frame, w0); break;
+            case prog::K_NQ: prog::nq_task(A, S, frame, w0); break;
+            case prog::K_CILKSORT:
+                if (kSorts) prog::cilksort_task(A, S, frame, w0, w1);
+                else { GTAP_ERROR(A, ERR_INVALID_KIND, tid, -1, kind, 0); rt_finish(S); }
+                break;
+            case prog::K_CILKMERGE:
+                if (kSorts) prog::cilkmerge_task(A, S, frame, w0, w1);
+                else { GTAP_ERROR(A, ERR_INVALID_KIND, tid, -1, kind, 0); rt_finish(S); }
+                break;
+            case prog::K_MERGESORT:
+                if (kSorts) prog::mergesort_task(A, S, frame, w0, w1);
+                else { GTAP_ERROR(A, ERR_INVALID_KIND, tid, -1, kind, 0); rt_finish(S); }
+                break;
+            case prog::K_BFS: prog::bfs_task(A, S, frame, w0); break;
+            case prog::K_TREESUM: prog::treesum_task(A, S, frame, w0, w1); break;
+            default:
+                GTAP_ERROR(A, ERR_INVALID_KIND, tid, -1, kind, 0);
+                rt_finish(S);
+                break;
+        }
+    }
+};
+
+using BuiltinProgram = BuiltinProgramT<true>;
+using BuiltinProgramLight = BuiltinProgramT<false>;
+
+}  // namespace gtap

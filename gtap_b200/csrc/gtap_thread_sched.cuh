@@ -1,0 +1,943 @@
+// gtap_thread_sched.cuh -- thread-executed mode: one task per CUDA thread,
+// one worker per warp, persistent kernel.
+//
+// Reference: runtime/detail/thread/gtap_runtime_thread.cuh (paths relative to
+// the reference project root).
+//   __gtap_execute_task_loop_device_impl :849-1040  -> worker_loop()
+//   pop_batch :511-536                              -> pop_own()
+//   steal_batch :538-593                            -> steal()
+//   push_batch :595-660                             -> finish_round() (select + publish)
+//   reserve_unpublished_task_id :38-48              -> stage_child()
+//   __gtap_spawn_task :768-816                      -> rt_spawn()
+//   __gtap_set_state_for_join :672-696              -> rt_join()
+//   __gtap_finish_task / notify_parent :714-764     -> rt_finish() + finish_round()
+//   get_task_id_from_warp_pool / release :111-146 (gtap_thread_core.cuh) -> id cache below
+//   termination :927-964                            -> per-root balances (no active-worker counter)
+//
+// Differences that matter for speed on B200:
+//   * the up-to-32 tasks a warp runs next stay in registers; only the surplus
+//     is written to the deque and published with ONE release add per queue;
+//   * no victim lock: steals claim a batch with one CAS on a packed
+//     (tag | bottom | top) word, and up to probe_width victims are probed in
+//     parallel by different lanes before choosing the fullest;
+//   * no __threadfence() per task: a finishing child performs one acq_rel
+//     decrement of the parent's join word, which also carries the queue the
+//     parent resumes on;
+//   * task ids come from a per-warp shared-memory cache refilled in batches of
+//     32 (private range, then the global recycled-id ring, then fresh ids);
+//   * termination: each warp holds pre-charged per-root balances, so the
+//     global per-root counter is touched once per ~kBalChunk tasks and a root
+//     completes exactly when its counter returns to zero.
+#pragma once
+#include "gtap_device.cuh"
+
+namespace gtap {
+
+constexpr int kAvailCap = 128;
+constexpr int kAvailLow = 48;
+constexpr int kAvailHigh = 96;
+constexpr int kFreedCap = 96;
+constexpr int kRootBalCap = 8;
+constexpr int kBalChunk = 1024;
+constexpr int kLocalCap = 128;     // per-warp, per-queue local ready stack (power of two)
+constexpr int kReserve = 32;       // ready tasks a warp keeps when others are hungry
+constexpr int kHungryReplicas = 8;  // copies of the hungry-worker count, 128 bytes apart
+constexpr int kHungryStride = 32;
+
+struct RootBal {
+    int root;
+    int bal;
+    int created;
+    int touched;
+};
+
+// Per-warp shared state.  This is the object the task ABI calls TaskContext.
+struct WarpShared {
+    int l_tid[kWarp];
+    int l_root[kWarp];
+    unsigned l_w0[kWarp];      // header word 0 of the running task: state | kind << 16 | flags << 24
+    int l_parent[kWarp];
+    int l_spawned[kWarp];      // children spawned since the last taskwait
+    int l_created[kWarp];      // tasks this lane created this round
+    int l_value[kWarp];        // contributions to the lane's root value (n-queens counts)
+    unsigned fin_mask;         // lanes whose task returned this round
+    unsigned retain_mask;      // finished lanes whose id the parent releases
+    unsigned spawn_mask;       // lanes that spawned this round
+    int cnt[kMaxQueues];       // children staged this round, per queue
+    unsigned bottom[kMaxQueues];
+    unsigned top_cache[kMaxQueues];
+    int cur_q;                 // EPAQ queue to try first (reference ctx->queue_idx)
+    int avail_n, alloc_pos, freed_n, bump;
+    int avail[kAvailCap];
+    int freed[kFreedCap];
+    int nbal;
+    RootBal bal[kRootBalCap];
+    unsigned long long st[GTAP_STAT_COUNT];
+    int worker;
+    int prof_h, prof_w;
+    int* sbuf;                 // [num_queues][spawn_cap] staged child ids (| spawner lane << 27)
+    int* lstk;                 // [num_queues][kLocalCap] ready tasks not yet visible to thieves
+    unsigned ls_lo[kMaxQueues];   // oldest entry (published first)
+    unsigned ls_hi[kMaxQueues];   // one past the newest entry (run first)
+};
+
+struct TaskCtxT {
+    const Arena* A;
+    WarpShared* S;
+};
+
+// ---------------------------------------------------------------------------
+// task-id allocation
+// ---------------------------------------------------------------------------
+__device__ __noinline__ int alloc_id_slow(const Arena& A, WarpShared& S) {
+    int b = atomicAdd(&S.bump, 1);
+    if (b < A.ids_per_worker) return S.worker * A.ids_per_worker + b;
+    unsigned f = atom_add_relaxed(A.fresh_next, 1u);
+    if (f < (unsigned)A.total_ids) return (int)f;
+    // recycled ids, one at a time (rare: the per-round refill keeps the cache full)
+    const Ring& r = A.idpool;
+    const unsigned cap = 1u << r.cap_log2;
+    for (int attempt = 0; attempt < 4096; ++attempt) {
+        unsigned h = ld_relaxed(r.head), t = ld_relaxed(r.tail);
+        if (t == h || t - h > cap) break;   // pool empty: every id is live
+        if (atom_cas_relaxed(r.head, h, h + 1) == h) {
+            unsigned want = ring_tag(r, h);
+            for (int spin = 0; spin < (1 << 20); ++spin) {
+                unsigned long long w = ld_acquire(&r.slots[h & (cap - 1)]);
+                if ((unsigned)(w >> 32) == want) return (int)(unsigned)(w & 0xFFFFFFFFu) - 1;
+                __nanosleep(64);
+            }
+            GTAP_ERROR(A, ERR_TIMEOUT, -1, -1, (int)h, 0);
+            return A.total_ids;
+        }
+        __nanosleep(32);
+    }
+    GTAP_ERROR(A, ERR_POOL_EXHAUSTED, -1, -1, A.total_ids, A.total_ids);
+    return A.total_ids;   // the spare record: written to, never staged or run
+}
+
+__device__ __forceinline__ int alloc_id(const Arena& A, WarpShared& S) {
+    int a = atomicAdd(&S.alloc_pos, 1);
+    if (a < S.avail_n) return S.avail[a];
+    return alloc_id_slow(A, S);
+}
+
+// Warp-cooperative: compact the cache after a round, return surplus ids to
+// the global ring and refill from the private range / ring / fresh ids.
+__device__ void id_cache_maintain(const Arena& A, WarpShared& S) {
+    const unsigned lane = lane_id();
+    __syncwarp();
+    int consumed = min(S.alloc_pos, S.avail_n);
+    int remain = S.avail_n - consumed;
+    int nfreed = min(S.freed_n, kFreedCap);
+    // move remaining entries to the front (read all, then write)
+    int v0 = 0, v1 = 0, v2 = 0, v3 = 0;
+    if ((int)lane < remain) v0 = S.avail[consumed + lane];
+    if ((int)lane + 32 < remain) v1 = S.avail[consumed + lane + 32];
+    if ((int)lane + 64 < remain) v2 = S.avail[consumed + lane + 64];
+    if ((int)lane + 96 < remain) v3 = S.avail[consumed + lane + 96];
+    __syncwarp();
+    if ((int)lane < remain) S.avail[lane] = v0;
+    if ((int)lane + 32 < remain) S.avail[lane + 32] = v1;
+    if ((int)lane + 64 < remain) S.avail[lane + 64] = v2;
+    if ((int)lane + 96 < remain) S.avail[lane + 96] = v3;
+    __syncwarp();
+    // append freed ids; whatever does not fit goes to the global ring
+    int n = remain;
+    for (int base = 0; base < nfreed; base += 32) {
+        int i = base + (int)lane;
+        int id = (i < nfreed) ? S.freed[i] : -1;
+        int take = min(32, nfreed - base);
+        int room = kAvailCap - n;
+        if (take <= room) {
+            if ((int)lane < take) S.avail[n + lane] = id;
+            n += take;
+        } else {
+            // push this chunk of freed ids to the recycled-id ring
+            ring_push_warp(A, A.idpool, id, take);
+        }
+        __syncwarp();
+    }
+    // surplus: give 32 back
+    if (n > kAvailHigh) {
+        int id = S.avail[n - 32 + lane];
+        __syncwarp();
+        ring_push_warp(A, A.idpool, id, 32);
+        n -= 32;
+    }
+    // refill
+    if (n < kAvailLow) {
+        int got = 0;
+        // private range first (no memory traffic)
+        int b = S.bump;
+        if (b < A.ids_per_worker) {
+            int k = min(32, A.ids_per_worker - b);
+            if ((int)lane < k) S.avail[n + lane] = S.worker * A.ids_per_worker + b + lane;
+            got = k;
+            __syncwarp();
+            if (lane == 0) S.bump = b + k;
+        }
+        if (got == 0) {
+            int id = -1;
+            got = ring_pop_warp(A, A.idpool, 32, &id);
+            if ((int)lane < got) S.avail[n + lane] = id;
+        }
+        if (got == 0) {
+            unsigned f = 0;
+            if (lane == 0) f = atom_add_relaxed(A.fresh_next, 32u);
+            f = __shfl_sync(0xffffffffu, f, 0);
+            if (f < (unsigned)A.total_ids) {
+                int k = min(32, A.total_ids - (int)f);
+                if ((int)lane < k) S.avail[n + lane] = (int)f + lane;
+                got = k;
+            }
+        }
+        n += got;
+    }
+    __syncwarp();
+    if (lane == 0) {
+        S.avail_n = n;
+        S.alloc_pos = 0;
+        S.freed_n = 0;
+    }
+    __syncwarp();
+}
+
+// ---------------------------------------------------------------------------
+// task ABI used by task bodies (one lane = one task)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int rt_state(const WarpShared& S) { return (int)(S.l_w0[lane_id()] & 0xFFFFu); }
+
+// Allocate a child, write its header, stage it for this round's push.
+// Children are invisible to other workers until the round ends
+// (reference contract of __gtap_spawn_task).
+__device__ __forceinline__ void* rt_spawn(const Arena& A, WarpShared& S, int kind, int q, int* child_count,
+                                          int* out_tid, bool retain, bool detached) {
+    const unsigned lane = lane_id();
+    if ((unsigned)q >= (unsigned)A.num_queues) {
+        GTAP_ERROR(A, ERR_INVALID_QUEUE_IDX, S.l_tid[lane], q, q, A.num_queues);
+        q = 0;
+    }
+    int id = alloc_id(A, S);
+    if (out_tid) *out_tid = id;
+    if (id >= A.total_ids) return frame_of(A, A.total_ids);   // allocation failed; error already recorded
+    TaskHeader* h = hdr_of(A, id);
+    int4 hw;
+    hw.x = (int)((unsigned)kind << 16 | (unsigned)(q | (retain ? kFlagRetain : 0)) << 24);
+    hw.y = detached ? -1 : S.l_tid[lane];
+    hw.z = 0;
+    hw.w = S.l_root[lane];
+    *reinterpret_cast<int4*>(h) = hw;
+    int s = atomicAdd(&S.cnt[q], 1);
+    if (s < A.spawn_cap) {
+        S.sbuf[q * A.spawn_cap + s] = id | (int)(lane << kIdBits);
+    } else {
+        GTAP_ERROR(A, ERR_SPAWN_BUFFER_OVERFLOW, S.l_tid[lane], q, s, A.spawn_cap);
+    }
+    if (child_count) ++*child_count;
+    if (!detached) S.l_spawned[lane] += 1;
+    S.l_created[lane] += 1;
+    return frame_of(A, id);
+}
+
+// taskwait: returns true if the task must suspend (children outstanding).
+__device__ __forceinline__ bool rt_join(const Arena& A, WarpShared& S, int child_count, int next_state, int q_after) {
+    const unsigned lane = lane_id();
+    if ((unsigned)q_after >= (unsigned)A.num_queues) {
+        GTAP_ERROR(A, ERR_INVALID_QUEUE_IDX_AFTER_JOIN, S.l_tid[lane], q_after, q_after, A.num_queues);
+        q_after = 0;
+    }
+    S.l_spawned[lane] = 0;
+    if (child_count == 0) {
+        S.l_w0[lane] = (S.l_w0[lane] & 0xFFFF0000u) | (unsigned)(next_state & 0xFFFF);
+        return false;
+    }
+    unsigned w0 = (S.l_w0[lane] & 0xFFFF0000u) | (unsigned)(next_state & 0xFFFF);
+    S.l_w0[lane] = w0;
+    int4 hw;
+    hw.x = (int)w0;
+    hw.y = S.l_parent[lane];
+    hw.z = (child_count & kJoinCountMask) | (q_after << 24);
+    hw.w = S.l_root[lane];
+    *reinterpret_cast<int4*>(hdr_of(A, S.l_tid[lane])) = hw;
+    return true;
+}
+
+// Task returned.  Parent notification and id release happen at round end.
+__device__ __forceinline__ void rt_finish(const WarpShared& S_, bool retain_override = false) {
+    WarpShared& S = const_cast<WarpShared&>(S_);
+    const unsigned lane = lane_id();
+    atomicOr(&S.fin_mask, 1u << lane);
+    unsigned flags = S.l_w0[lane] >> 24;
+    if ((flags & kFlagRetain) || retain_override) atomicOr(&S.retain_mask, 1u << lane);
+}
+
+__device__ __forceinline__ void rt_release_id(WarpShared& S, int tid) {
+    int f = atomicAdd(&S.freed_n, 1);
+    if (f < kFreedCap) S.freed[f] = tid;
+    // an overfull freed list loses the id until the next launch resets the arena
+}
+
+// ---------------------------------------------------------------------------
+// root accounting
+// ---------------------------------------------------------------------------
+__device__ void complete_root(const Arena& A, int r) {
+    gtap_root_result* res = &A.results[r];
+    res->t_done_ns = global_ns();
+    __threadfence();
+    st_release(&res->status, GTAP_ROOT_DONE);
+    unsigned c = atomicAdd(A.completed, 1u) + 1u;
+    if (A.mode == 2 /* serve */) {
+        if (A.done_ring) {
+            unsigned slot = (c - 1u) % A.done_ring_cap;
+            unsigned long long w = ((unsigned long long)(c - 1u) << 32) | (unsigned)(r + 1);
+            volatile unsigned long long* p = A.done_ring + slot;
+            *p = w;
+            __threadfence_system();
+        }
+    } else if (c >= (unsigned)A.n_roots) {
+        st_release(A.done_flag, 1);
+    }
+}
+
+// counter update; completes the root when it reaches zero
+__device__ __forceinline__ void outstanding_add(const Arena& A, int r, long long d) {
+    long long old = atom_add_acq_rel(&A.outstanding[r], d);
+    if (old + d == 0) complete_root(A, r);
+}
+
+__device__ void flush_bal(const Arena& A, RootBal& e) {
+    if (e.created) red_add_relaxed(reinterpret_cast<long long*>(&A.results[e.root].tasks), (long long)e.created);
+    e.created = 0;
+    if (e.bal != 0) outstanding_add(A, e.root, -(long long)e.bal);
+    e.bal = 0;
+}
+
+// lane 0 only
+__device__ void flush_all_bal(const Arena& A, WarpShared& S) {
+    for (int i = 0; i < S.nbal; ++i) flush_bal(A, S.bal[i]);
+    S.nbal = 0;
+}
+
+// Called by one leader lane per distinct root, serialised across leaders.
+__device__ void account_root(const Arena& A, WarpShared& S, int r, int created, int finished) {
+    int idx = -1;
+    for (int i = 0; i < S.nbal; ++i)
+        if (S.bal[i].root == r) { idx = i; break; }
+    if (idx < 0 && S.nbal < kRootBalCap) {
+        idx = S.nbal++;
+        S.bal[idx].root = r;
+        S.bal[idx].bal = 0;
+        S.bal[idx].created = 0;
+    }
+    if (idx < 0) {
+        // no cache slot: apply directly (creations before publication keep it safe)
+        if (created) red_add_relaxed(reinterpret_cast<long long*>(&A.results[r].tasks), (long long)created);
+        if (created != finished) outstanding_add(A, r, (long long)(created - finished));
+        return;
+    }
+    RootBal& e = S.bal[idx];
+    e.touched = 1;
+    e.created += created;
+    e.bal += finished - created;
+    if (e.bal < 0) {
+        int top = kBalChunk - e.bal;
+        outstanding_add(A, r, (long long)top);
+        e.bal = kBalChunk;
+    }
+}
+
+// lane 0: flush entries not touched this round so completions are seen promptly
+__device__ void age_bal(const Arena& A, WarpShared& S) {
+    int j = 0;
+    for (int i = 0; i < S.nbal; ++i) {
+        if (S.bal[i].touched) {
+            S.bal[i].touched = 0;
+            if (j != i) S.bal[j] = S.bal[i];
+            ++j;
+        } else {
+            flush_bal(A, S.bal[i]);
+        }
+    }
+    S.nbal = j;
+}
+
+// ---------------------------------------------------------------------------
+// deque operations
+// ---------------------------------------------------------------------------
+// Owner pop: LIFO, up to 32 newest published tasks of queue k.
+__device__ int pop_own(const Arena& A, WarpShared& S, int k, int& my_tid) {
+    const unsigned lane = lane_id();
+    if (((S.bottom[k] - S.top_cache[k]) & kPosMask) == 0) return 0;  // top only grows: surely empty
+    int got = 0;
+    unsigned b = 0;
+    if (lane == 0) {
+        unsigned long long* c = dq_ctl_ptr(A, k, S.worker);
+        unsigned long long wv = ld_relaxed(c);
+        for (int i = 0; i < 16; ++i) {
+            unsigned sz = dq_size(wv);
+            S.top_cache[k] = dq_top(wv);
+            if (sz == 0) break;
+            unsigned take = sz < 32u ? sz : 32u;
+            unsigned long long old = atom_cas_acquire(c, wv, dq_owner_pop(wv, take));
+            if (old == wv) {
+                got = (int)take;
+                b = dq_bottom(wv);
+                break;
+            }
+            wv = old;
+        }
+        if (got) {
+            S.bottom[k] = (b - (unsigned)got) & kPosMask;
+            S.st[GTAP_STAT_POPS] += 1;
+        }
+    }
+    got = __shfl_sync(0xffffffffu, got, 0);
+    b = __shfl_sync(0xffffffffu, b, 0);
+    if ((int)lane < got) my_tid = ld_relaxed(dq_slot_ptr(A, k, S.worker, b - (unsigned)got + lane));
+    return got;
+}
+
+__device__ __forceinline__ unsigned xorshift32(unsigned& s) {
+    s ^= s << 13;
+    s ^= s >> 17;
+    s ^= s << 5;
+    return s;
+}
+
+// Thief: probe up to probe_width random victims in parallel (one lane each),
+// take up to steal_batch (at most half) of the fullest one's queue k with one
+// CAS on its control word.
+__device__ int steal(const Arena& A, WarpShared& S, int k, unsigned& rng, int& last_victim, int& my_tid) {
+    const unsigned lane = lane_id();
+    const int W = A.num_workers;
+    if (W < 2) return 0;
+    int victim = -1;
+    unsigned long long wv = 0;
+    unsigned sz = 0;
+    if ((int)lane < A.probe_width) {
+        int v;
+        if (lane == 0 && A.victim_policy == GTAP_VICTIM_LAST_SUCCESS && last_victim >= 0) {
+            v = last_victim;
+        } else {
+            v = (int)(xorshift32(rng) % (unsigned)(W - 1));
+            if (v >= S.worker) ++v;
+        }
+        victim = v;
+        wv = ld_acquire(dq_ctl_ptr(A, k, v));
+        sz = dq_size(wv);
+    }
+    // argmax over lanes (largest size, lowest lane on ties)
+    unsigned key = (sz << 5) | (31u - lane);
+    if (sz > (1u << 21)) key = 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned other = __shfl_xor_sync(0xffffffffu, key, o);
+        key = other > key ? other : key;
+    }
+    if (lane == 0) S.st[GTAP_STAT_STEAL_ATTEMPTS] += 1;
+    if ((key >> 5) == 0) return 0;
+    int src = 31 - (int)(key & 31u);
+    victim = __shfl_sync(0xffffffffu, victim, src);
+    wv = __shfl_sync(0xffffffffu, wv, src);
+    unsigned long long* c = dq_ctl_ptr(A, k, victim);
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        unsigned size = dq_size(wv);
+        if (size == 0 || size > (1u << 20)) return 0;
+        unsigned t = dq_top(wv);
+        unsigned half = (size + 1u) >> 1;
+        unsigned n = half < (unsigned)A.steal_batch ? half : (unsigned)A.steal_batch;
+        int id = -1;
+        if (lane < n) id = ld_relaxed(dq_slot_ptr(A, k, victim, t + lane));
+        __syncwarp();
+        unsigned long long old = 0;
+        if (lane == 0) old = atom_cas_acquire(c, wv, dq_with_top(wv, t + n));
+        old = __shfl_sync(0xffffffffu, old, 0);
+        if (old == wv) {
+            if (lane < n) my_tid = id;
+            if (lane == 0) {
+                S.st[GTAP_STAT_STEAL_SUCCESSES] += 1;
+                S.st[GTAP_STAT_STOLEN_TASKS] += n;
+            }
+            last_victim = victim;
+            return (int)n;
+        }
+        wv = old;
+    }
+    return 0;
+}
+
+// Publish m entries src[(start + i) & mask] to this warp's deque of queue k
+// (thieves see them after the release add), spilling to the overflow queue
+// when the deque is full.
+__device__ void publish_src(const Arena& A, WarpShared& S, int k, const int* base, unsigned start, unsigned mask,
+                            int m) {
+    const unsigned lane = lane_id();
+    const unsigned cap = 1u << A.deque_cap_log2;
+    auto src = [&](int i) { return base[(start + (unsigned)i) & mask]; };
+    unsigned used = (S.bottom[k] - S.top_cache[k]) & kPosMask;
+    if (used + (unsigned)m > cap) {
+        unsigned long long wv = 0;
+        if (lane == 0) wv = ld_relaxed(dq_ctl_ptr(A, k, S.worker));
+        wv = __shfl_sync(0xffffffffu, wv, 0);
+        if (lane == 0) S.top_cache[k] = dq_top(wv);
+        __syncwarp();
+        used = (S.bottom[k] - S.top_cache[k]) & kPosMask;
+    }
+    int direct = m;
+    if (used + (unsigned)m > cap) direct = (int)(cap - used);
+    if (direct > 0) {
+        const unsigned b = S.bottom[k];
+        for (int e = (int)lane; e < direct; e += 32) *dq_slot_ptr(A, k, S.worker, b + (unsigned)e) = src(e) & kIdMask;
+        __syncwarp();
+        if (lane == 0) {
+            red_add_release(dq_ctl_ptr(A, k, S.worker), (unsigned long long)direct << kPosBits);
+            S.bottom[k] = (b + (unsigned)direct) & kPosMask;
+            S.st[GTAP_STAT_PUBLISHED] += (unsigned long long)direct;
+        }
+    }
+    // the rest spills to the global overflow queue
+    for (int base = direct; base < m; base += 32) {
+        int take = min(32, m - base);
+        int id = ((int)lane < take) ? (src(base + (int)lane) & kIdMask) : 0;
+        fence_acq_rel();
+        ring_push_warp(A, A.overflow, id, take);
+        if (lane == 0) S.st[GTAP_STAT_OVERFLOW_PUSHES] += (unsigned long long)take;
+    }
+    __syncwarp();
+}
+
+// ---------------------------------------------------------------------------
+// profiling (reference gtap_profile_thread.cuh timelines)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void prof_having(const Arena& A, WarpShared& S) {
+    if (A.prof_cap > 0 && lane_id() == 0 && S.prof_h < A.prof_cap) {
+        A.prof_having[(size_t)S.worker * A.prof_cap + S.prof_h] = (long long)global_ns();
+        S.prof_h++;
+    }
+}
+__device__ __forceinline__ void prof_working(const Arena& A, WarpShared& S, int nb) {
+    if (A.prof_cap > 0 && lane_id() == 0 && S.prof_w < A.prof_cap) {
+        size_t i = (size_t)S.worker * A.prof_cap + S.prof_w;
+        A.prof_working[i] = (long long)global_ns();
+        A.prof_tasks[i] = nb;
+        S.prof_w++;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// admission: claim roots from the root table (batch) or the published ring (serve)
+// ---------------------------------------------------------------------------
+template <class Prog>
+__device__ int admit(const Arena& A, WarpShared& S, int& my_tid) {
+    const unsigned lane = lane_id();
+    int first = 0, k = 0;
+    if (lane == 0) {
+        unsigned limit;
+        limit = (A.mode == 2) ? ld_acquire(A.published) : (unsigned)A.n_roots;
+        // admission by free task-frame memory: never-used + recycled ids
+        unsigned fresh = ld_relaxed(A.fresh_next);
+        unsigned pool = ld_relaxed(A.idpool.tail) - ld_relaxed(A.idpool.head);
+        long long free_ids = (long long)A.total_ids - (long long)fresh + (long long)pool;
+        if (free_ids < (long long)A.admit_watermark) limit = 0;
+        if (A.max_inflight > 0) {
+            // admitted - completed < max_inflight
+            const unsigned done = ld_relaxed(A.completed);
+            const unsigned cap = done + (unsigned)A.max_inflight;
+            if (cap < limit) limit = cap;
+        }
+        for (int attempt = 0; attempt < 8; ++attempt) {
+            unsigned c = ld_relaxed(A.next_root);
+            if (c >= limit) break;
+            unsigned take = limit - c;
+            if (take > (unsigned)A.admit_batch) take = (unsigned)A.admit_batch;
+            if (atom_cas_relaxed(A.next_root, c, c + take) == c) {
+                first = (int)c;
+                k = (int)take;
+                break;
+            }
+        }
+    }
+    k = __shfl_sync(0xffffffffu, k, 0);
+    first = __shfl_sync(0xffffffffu, first, 0);
+    if (k == 0) return 0;
+    if ((int)lane < k) {
+        int idx = first + (int)lane;
+        int slot = (A.mode == 2) ? (int)((unsigned)idx % (unsigned)A.n_roots) : idx;
+        const gtap_root& rd = A.roots[slot];
+        int id = alloc_id(A, S);
+        if (id >= A.total_ids) id = A.total_ids;   // error recorded; the launch aborts
+        int kind = Prog::root_kind(rd.kind);
+        if (kind < 0) {
+            GTAP_ERROR(A, ERR_INVALID_KIND, id, -1, rd.kind, GTAP_KIND_COUNT);
+            kind = 0;
+        }
+        TaskHeader* h = hdr_of(A, id);
+        int4 hw;
+        hw.x = (int)((unsigned)kind << 16);
+        hw.y = -1;
+        hw.z = 0;
+        hw.w = slot;
+        *reinterpret_cast<int4*>(h) = hw;
+        Prog::init_root(A, rd, frame_of(A, id));
+        gtap_root_result* res = &A.results[slot];
+        res->t_admit_ns = global_ns();
+        res->index = idx;
+        res->status = GTAP_ROOT_RUNNING;
+        // the root counts as one outstanding task from here on; its finish
+        // enters this or another warp's balance like any other task
+        atom_add_acq_rel(&A.outstanding[slot], 1ll);
+        red_add_relaxed(reinterpret_cast<long long*>(&res->tasks), 1ll);
+        S.l_created[lane] = 0;
+        S.l_root[lane] = slot;
+        my_tid = id;
+    }
+    __syncwarp();
+    if (lane == 0) S.st[GTAP_STAT_TASKS] += (unsigned long long)k;
+    return k;
+}
+
+// ---------------------------------------------------------------------------
+// the persistent worker loop
+// ---------------------------------------------------------------------------
+template <class Prog>
+__device__ void worker_loop(const Arena& A, WarpShared& S) {
+    const unsigned lane = lane_id();
+    int my_tid = -1;
+    int nb = 0;
+    unsigned rng = 0x9E3779B9u ^ (unsigned)(S.worker * 2654435761u) ^ (lane * 0x85EBCA6Bu) ^ (unsigned)clock64();
+    if (rng == 0) rng = 1;
+    int last_victim = -1;
+    int backoff = 0;
+    bool having = false;
+    const unsigned long long t_start = global_ns();
+    int round = 0;
+    bool idle = false;                       // counted in the hungry replicas
+    int* const hungry_mine = A.hungry + (S.worker % kHungryReplicas) * kHungryStride;
+    auto hungry_add = [&](int d) {
+        for (int r = 0; r < kHungryReplicas; ++r) red_add_relaxed_i32(A.hungry + r * kHungryStride, d);
+    };
+
+    for (;;) {
+        if (lane == 0) {
+            S.fin_mask = 0;
+            S.retain_mask = 0;
+        }
+        S.l_created[lane] = 0;
+        __syncwarp();
+
+        if (nb == 0) {
+            // acquire: own deque, then steal, per EPAQ queue starting at cur_q
+            // (reference :896-926), then the overflow queue, then new roots.
+            const int Q = A.num_queues;
+            for (int kk = 0; kk < Q && nb == 0; ++kk) {
+                int k = (S.cur_q + kk) % Q;
+                nb = pop_own(A, S, k, my_tid);
+                if (nb == 0) nb = steal(A, S, k, rng, last_victim, my_tid);
+                if (nb) {
+                    if (lane == 0) S.cur_q = k;
+                }
+            }
+            if (nb == 0) nb = ring_pop_warp(A, A.overflow, 32, &my_tid);
+            if (nb == 0) nb = admit<Prog>(A, S, my_tid);
+            __syncwarp();
+            if (nb == 0) {
+                if (having) {
+                    prof_having(A, S);
+                    having = false;
+                }
+                int stop = 0;
+                if (lane == 0) {
+                    if (!idle && A.publish_lazy) hungry_add(1);
+                    flush_all_bal(A, S);
+                    S.st[GTAP_STAT_IDLE_POLLS] += 1;
+                    if (ld_acquire(A.done_flag) != 0 || aborted(A)) stop = 1;
+                    if (A.mode == 2 && ld_relaxed(A.shutdown) != 0) {
+                        unsigned pub = ld_acquire(A.published);
+                        if (ld_acquire(A.completed) >= pub && ld_relaxed(A.next_root) >= pub) stop = 1;
+                    }
+                    if (!stop && global_ns() - t_start > A.watchdog_ns) {
+                        GTAP_ERROR(A, ERR_TIMEOUT, -1, -1, 0, 0);
+                        stop = 1;
+                    }
+                }
+                idle = true;
+                stop = __shfl_sync(0xffffffffu, stop, 0);
+                if (stop) break;
+                if (backoff < 6) ++backoff;
+                __nanosleep(32u << backoff);
+                continue;
+            }
+            if (idle && lane == 0 && A.publish_lazy) hungry_add(-1);
+            idle = false;
+            backoff = 0;
+            if (!having) {
+                prof_having(A, S);
+                having = true;
+            }
+        }
+
+        // ---- execute: lane i runs task my_tid ----
+        int hv = 0;
+        if (lane == 0 && A.publish_lazy) hv = ld_relaxed(hungry_mine);   // consumed at round end
+        prof_working(A, S, nb);
+        int4 hw = make_int4(0, -1, 0, 0), fw0 = make_int4(0, 0, 0, 0), fw1 = fw0;
+        int bad = 0;
+        if ((int)lane < nb) {
+            if ((unsigned)my_tid >= (unsigned)A.total_ids) {
+                bad = 1;
+            } else {
+                // header and the first 32 frame bytes in one round trip
+                const char* rec = A.records + (size_t)my_tid * A.rec_stride;
+                hw = ld_cg_v4(rec);
+                fw0 = ld_cg_v4(rec + 16);
+                if (A.rec_stride >= 48) fw1 = ld_cg_v4(rec + 32);
+                if ((unsigned)hw.w >= (unsigned)A.n_roots || hw.y < -1 || hw.y >= A.total_ids) bad = 2;
+            }
+            if (bad) GTAP_ERROR(A, ERR_INVALID_ARGUMENT, my_tid, -1, bad == 1 ? my_tid : hw.w, A.total_ids);
+        }
+        if (__any_sync(0xffffffffu, bad)) break;   // corrupted id or header: stop this worker, launch aborts
+        if ((int)lane < nb) {
+            S.l_tid[lane] = my_tid;
+            S.l_w0[lane] = (unsigned)hw.x;
+            S.l_parent[lane] = hw.y;
+            S.l_root[lane] = hw.w;
+            S.l_spawned[lane] = 0;
+            S.l_value[lane] = 0;
+            Prog::exec(A, S, (int)(((unsigned)hw.x >> 16) & 0xFFu), my_tid, frame_of(A, my_tid), fw0, fw1);
+        }
+        __syncwarp();
+        prof_working(A, S, nb);
+
+        // ---- round end ----
+        int nb_next = 0, next_tid = -1;
+        const unsigned fin = S.fin_mask;
+        const bool active = (int)lane < nb;
+        const bool my_fin = active && ((fin >> lane) & 1u);
+        const unsigned spawners = __ballot_sync(0xffffffffu, active && S.l_spawned[lane] > 0);
+        // (1) orphans: children of tasks that returned without a taskwait
+        if (fin & spawners) {
+            for (int q = 0; q < A.num_queues; ++q) {
+                const int n = min(S.cnt[q], A.spawn_cap);
+                const int* sb = S.sbuf + q * A.spawn_cap;
+                for (int e = (int)lane; e < n; e += 32) {
+                    unsigned ent = (unsigned)sb[e];
+                    unsigned sp = ent >> kIdBits;
+                    if ((fin & spawners) >> sp & 1u) st_relaxed(&hdr_of(A, (int)(ent & kIdMask))->parent, -1);
+                }
+            }
+            __syncwarp();
+        }
+        // (2) join: the last child re-enqueues its parent on the resume queue
+        if (my_fin) {
+            const int parent = S.l_parent[lane];
+            if (parent >= 0) {
+                int old = atom_add_acq_rel(&hdr_of(A, parent)->join, -1);
+                if ((old & kJoinCountMask) == 1) {
+                    int q = (old >> 24) & 7;
+                    if (q >= A.num_queues) q = 0;
+                    int s = atomicAdd(&S.cnt[q], 1);
+                    if (s < A.spawn_cap) S.sbuf[q * A.spawn_cap + s] = parent | (int)(lane << kIdBits);
+                    else GTAP_ERROR(A, ERR_SPAWN_BUFFER_OVERFLOW, parent, q, s, A.spawn_cap);
+                }
+            }
+            // (3) release the finished task's id unless its parent reads its frame
+            if (!((S.retain_mask >> lane) & 1u)) rt_release_id(S, my_tid);
+        }
+        // (4) per-root accounting, one leader per distinct root
+        {
+            const int created = active ? S.l_created[lane] : 0;
+            const int finished = my_fin ? 1 : 0;
+            const int value = active ? S.l_value[lane] : 0;
+            const int r = active ? S.l_root[lane] : -1;
+            const unsigned amask = __ballot_sync(0xffffffffu, active);
+            unsigned grp = __match_any_sync(0xffffffffu, r);
+            int c_sum = created, f_sum = finished, v_sum = value;
+            if (active) {
+                c_sum = (int)__reduce_add_sync(grp, (unsigned)created);
+                f_sum = (int)__reduce_add_sync(grp, (unsigned)finished);
+                v_sum = (int)__reduce_add_sync(grp, (unsigned)value);
+            }
+            const bool leader = active && ((unsigned)__ffs(grp) - 1u == lane);
+            unsigned leaders = __ballot_sync(0xffffffffu, leader);
+            (void)amask;
+            __syncwarp();
+            while (leaders) {
+                const unsigned l = (unsigned)__ffs(leaders) - 1u;
+                if (lane == l) {
+                    if (v_sum) atomicAdd(reinterpret_cast<unsigned long long*>(&A.results[r].value),
+                                         (unsigned long long)(long long)v_sum);
+                    account_root(A, S, r, c_sum, f_sum);
+                }
+                __syncwarp();
+                leaders &= leaders - 1u;
+            }
+            if (lane == 0) age_bal(A, S);
+            __syncwarp();
+        }
+        // (5) children join their queue's local stack (newest on top); the
+        //     busiest queue's newest <= 32 run next (reference push_batch keeps
+        //     the newest 32 of k_max); the oldest entries become visible to
+        //     thieves only when a stack overflows or some worker is hungry.
+        {
+            const int Q = A.num_queues;
+            // eager publication behaves as if some worker were always hungry
+            const int hungry = A.publish_lazy ? __shfl_sync(0xffffffffu, hv, 0) : 1;
+            const int reserve = A.publish_lazy ? kReserve : 0;
+            int kmax = -1, best = 0;
+            for (int k = 0; k < Q; ++k)
+                if (S.cnt[k] > best) {
+                    best = S.cnt[k];
+                    kmax = k;
+                }
+            for (int k = 0; k < Q; ++k) {
+                const int n = min(S.cnt[k], A.spawn_cap);
+                if (n == 0) continue;
+                const int* sb = S.sbuf + k * A.spawn_cap;
+                int* ls = S.lstk + k * kLocalCap;
+                const unsigned lo = S.ls_lo[k], hi = S.ls_hi[k];
+                const int size = (int)(hi - lo);
+                const int over = size + n - kLocalCap;
+                int from_sb = 0;
+                if (over > 0) {
+                    const int m1 = min(over, size);
+                    if (m1 > 0) publish_src(A, S, k, ls, lo, kLocalCap - 1, m1);
+                    from_sb = over - m1;
+                    if (from_sb > 0) publish_src(A, S, k, sb, 0, 0xFFFFFFFFu, from_sb);
+                    if (lane == 0) S.ls_lo[k] = lo + (unsigned)m1;
+                }
+                for (int e = from_sb + (int)lane; e < n; e += 32)
+                    ls[(hi + (unsigned)(e - from_sb)) & (kLocalCap - 1)] = sb[e] & kIdMask;
+                __syncwarp();
+                if (lane == 0) S.ls_hi[k] = hi + (unsigned)(n - from_sb);
+                __syncwarp();
+            }
+            int kn = kmax;
+            if (kn < 0) {
+                for (int kk = 0; kk < Q; ++kk) {
+                    const int k = (S.cur_q + kk) % Q;
+                    if (S.ls_hi[k] != S.ls_lo[k]) {
+                        kn = k;
+                        break;
+                    }
+                }
+            }
+            nb_next = 0;
+            if (kn >= 0) {
+                int* ls = S.lstk + kn * kLocalCap;
+                const unsigned lo = S.ls_lo[kn], hi = S.ls_hi[kn];
+                const int size = (int)(hi - lo);
+                const int take = min(32, size);
+                nb_next = take;
+                if ((int)lane < take) next_tid = ls[(hi - (unsigned)take + lane) & (kLocalCap - 1)];
+                __syncwarp();
+                if (lane == 0) {
+                    S.ls_hi[kn] = hi - (unsigned)take;
+                    S.cur_q = kn;
+                }
+                __syncwarp();
+            }
+            if (hungry > 0) {
+                // keep one more batch in reserve so the next rounds stay full
+                for (int k = 0; k < Q; ++k) {
+                    const unsigned lo = S.ls_lo[k], hi = S.ls_hi[k];
+                    const int size = (int)(hi - lo);
+                    const int m = size - reserve;
+                    if (m > 0) {
+                        publish_src(A, S, k, S.lstk + k * kLocalCap, lo, kLocalCap - 1, m);
+                        if (lane == 0) S.ls_lo[k] = lo + (unsigned)m;
+                        __syncwarp();
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        if (lane == 0) {
+            for (int k = 0; k < A.num_queues; ++k) S.cnt[k] = 0;
+            S.st[GTAP_STAT_EXECUTIONS] += (unsigned long long)nb;
+            S.st[GTAP_STAT_ROUNDS] += 1;
+        }
+        const unsigned created_all = __reduce_add_sync(0xffffffffu, (unsigned)(active ? S.l_created[lane] : 0));
+        if (lane == 0) S.st[GTAP_STAT_TASKS] += created_all;
+        // (6) id cache
+        id_cache_maintain(A, S);
+        nb = nb_next;
+        my_tid = next_tid;
+        next_tid = -1;
+        // periodic abort / watchdog check while busy
+        if ((++round & 63) == 0) {
+            int stop = 0;
+            if (lane == 0) {
+                if (aborted(A)) stop = 1;
+                else if (global_ns() - t_start > A.watchdog_ns) {
+                    GTAP_ERROR(A, ERR_TIMEOUT, -1, -1, 1, 0);
+                    stop = 1;
+                }
+            }
+            if (__shfl_sync(0xffffffffu, stop, 0)) break;
+        }
+    }
+    if (lane == 0) flush_all_bal(A, S);
+}
+
+// Kernel: warps_per_block WarpShared records + staging buffers in dynamic smem.
+template <class Prog>
+__device__ __forceinline__ void thread_worker_body(const Arena& A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int wib = threadIdx.x >> 5;
+    const unsigned lane = lane_id();
+    WarpShared* ws = reinterpret_cast<WarpShared*>(smem_raw);
+    int* sb_base = reinterpret_cast<int*>(smem_raw + sizeof(WarpShared) * A.warps_per_block);
+    int* ls_base = sb_base + (size_t)A.warps_per_block * A.num_queues * A.spawn_cap;
+    WarpShared& S = ws[wib];
+    const int worker = blockIdx.x * A.warps_per_block + wib;
+    if (lane == 0) {
+        S.worker = worker;
+        S.sbuf = sb_base + (size_t)wib * A.num_queues * A.spawn_cap;
+        S.lstk = ls_base + (size_t)wib * A.num_queues * kLocalCap;
+        for (int k = 0; k < kMaxQueues; ++k) {
+            S.ls_lo[k] = 0;
+            S.ls_hi[k] = 0;
+            S.cnt[k] = 0;
+            S.bottom[k] = 0;
+            S.top_cache[k] = 0;
+        }
+        S.cur_q = 0;
+        S.alloc_pos = 0;
+        S.freed_n = 0;
+        S.nbal = 0;
+        S.prof_h = 0;
+        S.prof_w = 0;
+        S.fin_mask = 0;
+        S.retain_mask = 0;
+        for (int i = 0; i < GTAP_STAT_COUNT; ++i) S.st[i] = 0;
+    }
+    // first ids come from the private range
+    const int first = min(64, A.ids_per_worker);
+    if ((int)lane < first) S.avail[lane] = worker * A.ids_per_worker + (int)lane;
+    if ((int)lane + 32 < first) S.avail[lane + 32] = worker * A.ids_per_worker + (int)lane + 32;
+    if (lane == 0) {
+        S.avail_n = first;
+        S.bump = first;
+    }
+    __syncwarp();
+    worker_loop<Prog>(A, S);
+    __syncwarp();
+    if ((int)lane < GTAP_STAT_COUNT) A.stats[(size_t)worker * GTAP_STAT_COUNT + lane] = S.st[lane];
+}
+
+
+// Register-unbounded kernel (sorting kinds need the 64-key register network).
+template <class Prog>
+__global__ void thread_worker_kernel(const Arena A) {
+    thread_worker_body<Prog>(A);
+}
+
+// At most 64 registers per thread: any block size up to 1024 fits, and the
+// light program reaches 32 resident warps per SM.
+template <class Prog>
+__global__ void __launch_bounds__(1024, 1) thread_worker_kernel_lb(const Arena A) {
+    thread_worker_body<Prog>(A);
+}
+
+}  // namespace gtap
