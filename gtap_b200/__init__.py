@@ -17,6 +17,11 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libgtap_b200.so")
+if os.environ.get("GTAP_LIB_PATH"):
+    LIB_PATH = os.environ["GTAP_LIB_PATH"]   # an alternative build of the same library
+elif os.environ.get("GTAP_LIB_VARIANT") == "debug":
+    # same library built with per-id live checks (python -m gtap_b200.build --debug)
+    LIB_PATH = os.path.join(HERE, "libgtap_b200_debug.so")
 
 # ---- constants mirrored from include/gtap.h --------------------------------
 MODE_THREAD, MODE_BLOCK = 0, 1
@@ -123,6 +128,8 @@ _SIGS = [
     ("gtap_serve_shutdown", ctypes.c_int, [ctypes.POINTER(RunStats)]),
     ("gtap_visualize_profile", ctypes.c_int, [ctypes.c_char_p]),
     ("gtap_write_profile", ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p]),
+    ("gtap_selftest_queues", ctypes.c_int,
+     [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32] + [ctypes.POINTER(ctypes.c_int64)] * 4),
     ("gtap_gen_keys", ctypes.c_int, [ctypes.c_uint32, ctypes.c_void_p, ctypes.c_int64]),
     ("gtap_gen_mix", ctypes.c_int, [ctypes.c_uint64, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("gtap_gen_rmat", ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p]),
@@ -303,6 +310,13 @@ def serve_shutdown():
     rc = lib().gtap_serve_shutdown(ctypes.byref(st))
     _check(rc, "gtap_serve_shutdown")
     return st
+
+
+def selftest_queues(rounds=60, per_round_max=32, mode=7):
+    """Device exactly-once test of the deques and the overflow queue."""
+    v = [ctypes.c_int64(0) for _ in range(4)]
+    rc = lib().gtap_selftest_queues(rounds, per_round_max, mode, *[ctypes.byref(x) for x in v])
+    return rc, dict(zip(("produced", "consumed", "duplicates", "lost"), [x.value for x in v]))
 
 
 # ---- generators ----------------------------------------------------------------

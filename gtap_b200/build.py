@@ -10,6 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgtap_b200.so")
+LIB_DEBUG = os.path.join(HERE, "libgtap_b200_debug.so")
 
 NVCC_FLAGS = [
     "-O3", "-std=c++17",
@@ -40,20 +41,23 @@ def up_to_date():
     return all(os.path.getmtime(p) <= t for p in deps())
 
 
-def build(force=False, verbose=False):
-    if not force and up_to_date():
+def build(force=False, verbose=False, debug=False):
+    """Compile the library; debug=True builds libgtap_b200_debug.so with
+    per-task-id live checks (every violation is reported as a runtime error)."""
+    out = LIB_DEBUG if debug else LIB
+    if not force and not debug and up_to_date():
         return LIB
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-o", LIB] + sources()
+    cmd = ([nvcc] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose else []) + (["-DGTAP_DEBUG_IDS"] if debug else [])
+           + ["-o", out] + sources())
     r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
         raise RuntimeError("nvcc failed building libgtap_b200.so")
     if verbose:
         sys.stderr.write(r.stderr)
-    return LIB
+    return out
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose="-v" in sys.argv)
-    print(LIB)
+    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv, debug="--debug" in sys.argv))

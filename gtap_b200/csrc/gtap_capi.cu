@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "gtap_programs.cuh"
+#include "gtap_selftest.cuh"
 
 using namespace gtap;
 
@@ -53,6 +54,7 @@ struct Runtime {
     unsigned long long* ring_slots = nullptr;   // overflow ring followed by id pool ring
     unsigned* counters = nullptr;               // small device counters, see kCtr*
     int* hungry = nullptr;                      // kHungryReplicas x kHungryStride
+    int* dbg = nullptr;                         // debug builds: 2 x total_ids flags
     unsigned long long* stats = nullptr;
     long long* prof_having = nullptr;
     long long* prof_working = nullptr;
@@ -239,6 +241,9 @@ Arena make_arena(int n_roots, int mode, int workers) {
     A.report = g.d_report;
     A.stats = g.stats;
     A.hungry = g.hungry;
+    A.dbg_live = g.dbg;
+    A.dbg_exec = g.dbg ? g.dbg + c.total_ids : nullptr;
+    A.dbg_slotpos = g.dbg ? reinterpret_cast<unsigned*>(g.dbg + 2 * c.total_ids) : nullptr;
     A.prof_having = g.prof_having;
     A.prof_working = g.prof_working;
     A.prof_tasks = g.prof_tasks;
@@ -300,6 +305,7 @@ void free_all() {
     F(g.ring_slots);
     F(g.counters);
     F(g.hungry);
+    F(g.dbg);
     F(g.stats);
     F(g.prof_having);
     F(g.prof_working);
@@ -349,6 +355,11 @@ int launch_resident(int n_roots, cudaStream_t s, float* ms_out, bool light) {
         GT_CUDA(cudaMemsetAsync(g.prof_tasks, 0, n * sizeof(int), s));
     }
     ++g.epoch;
+#ifdef GTAP_DEBUG_IDS
+    GT_CUDA(cudaMemsetAsync(g.dbg, 0, (size_t)2 * g.cfg.total_ids * sizeof(int), s));
+    GT_CUDA(cudaMemsetAsync(g.dbg + 2 * g.cfg.total_ids, 0xFF,
+                            (size_t)g.cfg.num_queues * g.workers * g.cfg.deque_capacity * sizeof(int), s));
+#endif
     const int W = light ? g.workers_light : g.workers_full;
     g.last_workers = W;
     Arena A = make_arena(n_roots, 0, W);
@@ -382,7 +393,11 @@ int launch_resident(int n_roots, cudaStream_t s, float* ms_out, bool light) {
 // ===========================================================================
 extern "C" {
 
+#ifdef GTAP_DEBUG_IDS
+const char* gtap_version(void) { return "gtap_b200 0.1 (sm_100a, id checks)"; }
+#else
 const char* gtap_version(void) { return "gtap_b200 0.1 (sm_100a)"; }
+#endif
 
 int gtap_default_config(gtap_config* cfg) {
     if (!cfg) return GTAP_ERROR_INVALID_ARGUMENT;
@@ -462,6 +477,9 @@ int gtap_initialize(const gtap_config* cfg_in) {
     GT_CUDA(cudaMemset(g.counters, 0, kCtrCount * sizeof(unsigned)));
     GT_CUDA(cudaMalloc(&g.hungry, kHungryReplicas * kHungryStride * sizeof(int)));
     GT_CUDA(cudaMemset(g.hungry, 0, kHungryReplicas * kHungryStride * sizeof(int)));
+#ifdef GTAP_DEBUG_IDS
+    GT_CUDA(cudaMalloc(&g.dbg, ((size_t)2 * c.total_ids + (size_t)c.num_queues * g.workers * c.deque_capacity) * sizeof(int)));
+#endif
     GT_CUDA(cudaMalloc(&g.stats, (size_t)g.workers * GTAP_STAT_COUNT * sizeof(unsigned long long)));
     if (c.profile_samples > 0) {
         size_t n = (size_t)g.workers * c.profile_samples;
@@ -1051,4 +1069,71 @@ extern "C" int gtap_gen_tree(int32_t n, uint64_t seed, int32_t* left, int32_t* r
         size[p] = ps[i];
     }
     return 0;
+}
+
+// ---------------------------------------------------------------------------
+// queue self-test
+// ---------------------------------------------------------------------------
+namespace {
+__global__ void selftest_count_kernel(const unsigned* seen, size_t n, unsigned long long* ones,
+                                      unsigned long long* dups) {
+    unsigned long long o = 0, d = 0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        unsigned v = seen[i];
+        o += (v == 1u);
+        d += (v > 1u) ? (v - 1u) : 0u;
+    }
+    atomicAdd(ones, o);
+    atomicAdd(dups, d);
+}
+}  // namespace
+
+extern "C" int gtap_selftest_queues(int32_t rounds, int32_t per_round_max, int32_t mode, int64_t* produced,
+                                    int64_t* consumed, int64_t* duplicates, int64_t* lost) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g.initialized) return GTAP_ERROR_NOT_INITIALIZED;
+    if (g.serving) return GTAP_ERROR_BUSY;
+    if (rounds < 1 || per_round_max < 0 || per_round_max > g.cfg.spawn_capacity || mode < 0 || mode > 7)
+        return GTAP_ERROR_INVALID_ARGUMENT;
+    const int W = g.workers_light;
+    const size_t ntok = (size_t)W * 16384;
+    // every token may sit in the overflow ring at once: keep the volume below its capacity
+    if ((long long)rounds * per_round_max > 16383 ||
+        (long long)W * rounds * per_round_max > (1ll << g.overflow_log2))
+        return GTAP_ERROR_INVALID_ARGUMENT;
+    unsigned* seen = nullptr;
+    SelftestCounters* ctr = nullptr;
+    unsigned long long* sums = nullptr;
+    GT_CUDA(cudaMalloc(&seen, ntok * sizeof(unsigned)));
+    GT_CUDA(cudaMemset(seen, 0, ntok * sizeof(unsigned)));
+    GT_CUDA(cudaMalloc(&ctr, sizeof(SelftestCounters)));
+    GT_CUDA(cudaMemset(ctr, 0, sizeof(SelftestCounters)));
+    GT_CUDA(cudaMalloc(&sums, 2 * sizeof(unsigned long long)));
+    GT_CUDA(cudaMemset(sums, 0, 2 * sizeof(unsigned long long)));
+    ++g.epoch;
+    Arena A = make_arena(1, 0, W);
+    reset_kernel<<<64, 256>>>(A, g.counters, 1, W * g.cfg.ids_per_worker);
+    GT_CUDA(cudaGetLastError());
+    GT_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(&selftest_queue_kernel),
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem_bytes));
+    selftest_queue_kernel<<<W / g.warps_per_block, g.cfg.block, g.smem_bytes>>>(A, rounds, per_round_max, seen, ctr,
+                                                                                 mode);
+    GT_CUDA(cudaGetLastError());
+    selftest_count_kernel<<<1184, 256>>>(seen, ntok, sums, sums + 1);
+    GT_CUDA(cudaDeviceSynchronize());
+    SelftestCounters hc{};
+    unsigned long long hs[2] = {0, 0};
+    GT_CUDA(cudaMemcpy(&hc, ctr, sizeof(hc), cudaMemcpyDeviceToHost));
+    GT_CUDA(cudaMemcpy(hs, sums, sizeof(hs), cudaMemcpyDeviceToHost));
+    cudaFree(seen);
+    cudaFree(ctr);
+    cudaFree(sums);
+    const long long ones = (long long)hs[0], dups = (long long)hs[1];
+    if (produced) *produced = hc.produced;
+    if (consumed) *consumed = hc.consumed;
+    if (duplicates) *duplicates = dups + hc.bad_tokens;
+    if (lost) *lost = (long long)hc.produced - ones;
+    int st = read_status();
+    if (st) return st;
+    return (dups == 0 && hc.bad_tokens == 0 && ones == (long long)hc.produced) ? 0 : GTAP_ERROR_QUEUE_OVERFLOW;
 }

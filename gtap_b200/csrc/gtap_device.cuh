@@ -108,6 +108,35 @@ __device__ __forceinline__ int4 ld_cg_v4(const void* p) {
                  : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p) : "memory");
     return v;
 }
+// Loads of data written with plain stores (task records, sort buffers).
+// Readers on the writer's SM see the writes through L1; readers on other SMs
+// reach them only through an acquire (steal, pop, overflow ring, join), which
+// also drops stale L1 lines.  GTAP_RECORD_LOAD selects the load flavour.
+#ifndef GTAP_RECORD_LOAD
+#define GTAP_RECORD_LOAD 1
+#endif
+__device__ __forceinline__ int4 ld_data_v4(const void* p) {
+#if GTAP_RECORD_LOAD == 0
+    int4 v;
+    asm volatile("ld.global.cg.v4.s32 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p) : "memory");
+    return v;
+#else
+    int4 v;
+    asm volatile("ld.global.v4.s32 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p) : "memory");
+    return v;
+#endif
+}
+__device__ __forceinline__ int ld_data(const int* p) {
+    int v;
+#if GTAP_RECORD_LOAD == 0
+    asm volatile("ld.global.cg.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+#else
+    asm volatile("ld.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+#endif
+    return v;
+}
 __device__ __forceinline__ int ld_cg(const int* p) {
     int v;
     asm volatile("ld.global.cg.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -279,6 +308,11 @@ struct Arena {
     int* abort_flag;
     int* done_flag;
     GtapErrorReport* report;           // host-mapped report (may be null)
+
+    // debug builds (GTAP_DEBUG_IDS): live flag and fresh-execution flag per id
+    int* dbg_live;
+    int* dbg_exec;
+    unsigned* dbg_slotpos;   // position each deque slot was last written for
 
     // count of idle workers, replicated (see kHungryReplicas); busy workers
     // publish part of their local work while it is non-zero

@@ -92,7 +92,7 @@ __device__ __forceinline__ void fib_task(const Arena& A, WarpShared& S, void* fr
                 rt_spawn(A, S, K_FIB, epaq ? ((n - 2) < cutoff ? 1 : 0) : 0, &cc, nullptr, false, false));
             *reinterpret_cast<int4*>(c2) = make_int4(n - 2, 0, 0, 8);
             if (rt_join(A, S, cc, 1, epaq ? 2 : 0)) return;
-            fr = ld_cg_v4(f);
+            fr = ld_data_v4(f);
         }
         // fallthrough
         case 1: {
@@ -176,7 +176,7 @@ static_assert(sizeof(SortFrame) <= kFrameBytes && sizeof(MergeFrame) <= kFrameBy
 __device__ __noinline__ void sort_small(const int* in, int* out, int n) {
     int buf[64];
 #pragma unroll
-    for (int i = 0; i < 64; ++i) buf[i] = (i < n) ? ld_cg(in + i) : 0x7fffffff;
+    for (int i = 0; i < 64; ++i) buf[i] = (i < n) ? ld_data(in + i) : 0x7fffffff;
 #pragma unroll
     for (int k = 2; k <= 64; k <<= 1) {
 #pragma unroll
@@ -202,18 +202,18 @@ __device__ __noinline__ void sort_small(const int* in, int* out, int n) {
 // cilksort.cu:17-36
 __device__ __noinline__ void merge_seq(const int* a, int alen, const int* b, int blen, int* dst) {
     int i = 0, j = 0, k = 0;
-    int av = (alen > 0) ? ld_cg(a) : 0, bv = (blen > 0) ? ld_cg(b) : 0;
+    int av = (alen > 0) ? ld_data(a) : 0, bv = (blen > 0) ? ld_data(b) : 0;
     while (i < alen && j < blen) {
         if (av < bv) {
             dst[k++] = av;
-            if (++i < alen) av = ld_cg(a + i);
+            if (++i < alen) av = ld_data(a + i);
         } else {
             dst[k++] = bv;
-            if (++j < blen) bv = ld_cg(b + j);
+            if (++j < blen) bv = ld_data(b + j);
         }
     }
-    while (i < alen) dst[k++] = ld_cg(a + i++);
-    while (j < blen) dst[k++] = ld_cg(b + j++);
+    while (i < alen) dst[k++] = ld_data(a + i++);
+    while (j < blen) dst[k++] = ld_data(b + j++);
 }
 
 // cilksort.cu:38-49: largest index with x[idx] <= val
@@ -221,7 +221,7 @@ __device__ __forceinline__ int bsearch_le(const int* x, int len, int val) {
     int low = -1, high = len;
     while (low + 1 < high) {
         int mid = (low + high) / 2;
-        if (ld_cg(x + mid) <= val) low = mid;
+        if (ld_data(x + mid) <= val) low = mid;
         else high = mid;
     }
     return low;
@@ -255,7 +255,7 @@ __device__ __forceinline__ void cilkmerge_task(const Arena& A, WarpShared& S, vo
         int tl = alen; alen = blen; blen = tl;
     }
     if (blen == 0) {
-        for (int i = 0; i < alen; ++i) dst[i] = ld_cg(a + i);
+        for (int i = 0; i < alen; ++i) dst[i] = ld_data(a + i);
         rt_finish(S);
         return;
     }
@@ -266,7 +266,7 @@ __device__ __forceinline__ void cilkmerge_task(const Arena& A, WarpShared& S, vo
         return;
     }
     const int as = (alen + 1) / 2;
-    const int bs = bsearch_le(b, blen, ld_cg(a + as - 1)) + 1;
+    const int bs = bsearch_le(b, blen, ld_data(a + as - 1)) + 1;
     int cc = 0;
     spawn_merge(A, S, &cc, a, as, b, bs, dst);
     spawn_merge(A, S, &cc, a + as, alen - as, b + bs, blen - bs, dst + as + bs);
@@ -518,8 +518,8 @@ __device__ __forceinline__ void treesum_task(const Arena& A, WarpShared& S, void
                 *reinterpret_cast<int4*>(c) = make_int4(r, 16, 0, 0);
             }
             if (rt_join(A, S, cc, 1, 0)) return;
-            w0 = ld_cg_v4(frame);   // no child spawned: a, b are the zeros stored above
-            w1 = ld_cg_v4(reinterpret_cast<const char*>(frame) + 16);
+            w0 = ld_data_v4(frame);   // no child spawned: a, b are the zeros stored above
+            w1 = ld_data_v4(reinterpret_cast<const char*>(frame) + 16);
         }
         // fallthrough
         case 1: {
@@ -588,7 +588,7 @@ struct BuiltinProgramT {
             case GTAP_KIND_BFS: {
                 // asynchronous_bfs_thread.cu:51-55: depth[source] = 0 before the entry task
                 int* depth = reinterpret_cast<int*>(rd.p2);
-                depth[rd.i0] = 0;
+                atomicExch(depth + rd.i0, 0);   // depth is otherwise only touched by atomics and L2 loads
                 f[0] = make_int4(rd.i0, -1, -1, 0);
                 break;
             }

@@ -221,6 +221,10 @@ __device__ __forceinline__ void* rt_spawn(const Arena& A, WarpShared& S, int kin
     int id = alloc_id(A, S);
     if (out_tid) *out_tid = id;
     if (id >= A.total_ids) return frame_of(A, A.total_ids);   // allocation failed; error already recorded
+#ifdef GTAP_DEBUG_IDS
+    if (atomicExch(&A.dbg_live[id], 1) != 0) GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, id, q, 1, S.l_tid[lane]);
+    atomicExch(&A.dbg_exec[id], 0);
+#endif
     TaskHeader* h = hdr_of(A, id);
     int4 hw;
     hw.x = (int)((unsigned)kind << 16 | (unsigned)(q | (retain ? kFlagRetain : 0)) << 24);
@@ -270,6 +274,15 @@ __device__ __forceinline__ void rt_finish(const WarpShared& S_, bool retain_over
     atomicOr(&S.fin_mask, 1u << lane);
     unsigned flags = S.l_w0[lane] >> 24;
     if ((flags & kFlagRetain) || retain_override) atomicOr(&S.retain_mask, 1u << lane);
+}
+
+__device__ __forceinline__ void rt_release_id_dbg(const Arena& A, int tid) {
+#ifdef GTAP_DEBUG_IDS
+    if (atomicExch(&A.dbg_live[tid], 0) != 1) GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, tid, -1, 2, 0);
+#else
+    (void)A;
+    (void)tid;
+#endif
 }
 
 __device__ __forceinline__ void rt_release_id(WarpShared& S, int tid) {
@@ -383,6 +396,12 @@ __device__ int pop_own(const Arena& A, WarpShared& S, int k, int& my_tid) {
             if (old == wv) {
                 got = (int)take;
                 b = dq_bottom(wv);
+#ifdef GTAP_QUEUE_CHECKS
+                if (take > sz || sz > (1u << A.deque_cap_log2)) GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, (int)take, k, 23, (int)sz);
+#endif
+#ifdef GTAP_DEBUG_IDS
+                if (b != S.bottom[k]) GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, (int)b, k, 11, (int)S.bottom[k]);
+#endif
                 break;
             }
             wv = old;
@@ -394,7 +413,15 @@ __device__ int pop_own(const Arena& A, WarpShared& S, int k, int& my_tid) {
     }
     got = __shfl_sync(0xffffffffu, got, 0);
     b = __shfl_sync(0xffffffffu, b, 0);
-    if ((int)lane < got) my_tid = ld_relaxed(dq_slot_ptr(A, k, S.worker, b - (unsigned)got + lane));
+    if ((int)lane < got) {
+        my_tid = ld_relaxed(dq_slot_ptr(A, k, S.worker, b - (unsigned)got + lane));
+#ifdef GTAP_DEBUG_IDS
+        const unsigned pos = (b - (unsigned)got + lane) & kPosMask;
+        const size_t si = dq_slot_ptr(A, k, S.worker, pos) - A.dq_slots;
+        if (ld_cg((const int*)&A.dbg_slotpos[si]) != (int)pos)
+            GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, my_tid, k, 12, (int)pos);
+#endif
+    }
     return got;
 }
 
@@ -440,6 +467,7 @@ __device__ int steal(const Arena& A, WarpShared& S, int k, unsigned& rng, int& l
     int src = 31 - (int)(key & 31u);
     victim = __shfl_sync(0xffffffffu, victim, src);
     wv = __shfl_sync(0xffffffffu, wv, src);
+    __syncwarp();   // orders the probing lane's acquire before every lane's slot reads
     unsigned long long* c = dq_ctl_ptr(A, k, victim);
     for (int attempt = 0; attempt < 3; ++attempt) {
         unsigned size = dq_size(wv);
@@ -448,12 +476,33 @@ __device__ int steal(const Arena& A, WarpShared& S, int k, unsigned& rng, int& l
         unsigned half = (size + 1u) >> 1;
         unsigned n = half < (unsigned)A.steal_batch ? half : (unsigned)A.steal_batch;
         int id = -1;
-        if (lane < n) id = ld_relaxed(dq_slot_ptr(A, k, victim, t + lane));
+#ifdef GTAP_DEBUG_IDS
+        int shadow_ok = 1;
+#endif
+        if (lane < n) {
+            // Acquire: the read must be complete before lane 0's CAS claims the
+            // batch.  Once the CAS lands the owner may refill this slot for the
+            // next lap, and a relaxed load still in flight could return that
+            // newer value (a barrier alone does not wait for pending loads).
+            id = ld_acquire(dq_slot_ptr(A, k, victim, t + lane));
+#ifdef GTAP_DEBUG_IDS
+            const unsigned pos = (t + lane) & kPosMask;
+            const size_t si = dq_slot_ptr(A, k, victim, pos) - A.dq_slots;
+            shadow_ok = ld_cg((const int*)&A.dbg_slotpos[si]) == (int)pos;
+#endif
+        }
         __syncwarp();
         unsigned long long old = 0;
         if (lane == 0) old = atom_cas_acquire(c, wv, dq_with_top(wv, t + n));
         old = __shfl_sync(0xffffffffu, old, 0);
         if (old == wv) {
+#ifdef GTAP_DEBUG_IDS
+            if (lane < n && !shadow_ok) GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, id, k, 13, (int)((t + lane) & kPosMask));
+#endif
+#ifdef GTAP_QUEUE_CHECKS
+            if (lane == 0 && (n > size || size > (1u << A.deque_cap_log2)))
+                GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, (int)n, k, 22, (int)size);
+#endif
             if (lane < n) my_tid = id;
             if (lane == 0) {
                 S.st[GTAP_STAT_STEAL_SUCCESSES] += 1;
@@ -486,12 +535,39 @@ __device__ void publish_src(const Arena& A, WarpShared& S, int k, const int* bas
     }
     int direct = m;
     if (used + (unsigned)m > cap) direct = (int)(cap - used);
+#ifdef GTAP_QUEUE_CHECKS
+    if (lane == 0 && used > cap) GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, (int)used, k, 20, (int)cap);
+#endif
     if (direct > 0) {
         const unsigned b = S.bottom[k];
-        for (int e = (int)lane; e < direct; e += 32) *dq_slot_ptr(A, k, S.worker, b + (unsigned)e) = src(e) & kIdMask;
+#ifdef GTAP_QUEUE_CHECKS
+        if (lane == 0) {
+            unsigned long long w = ld_relaxed(dq_ctl_ptr(A, k, S.worker));
+            if (dq_bottom(w) != b) GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, (int)dq_bottom(w), k, 21, (int)b);
+            if (((b - dq_top(w)) & kPosMask) + (unsigned)direct > cap)
+                GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, (int)dq_top(w), k, 24, (int)S.top_cache[k]);
+        }
+#endif
+        for (int e = (int)lane; e < direct; e += 32) {
+            *dq_slot_ptr(A, k, S.worker, b + (unsigned)e) = src(e) & kIdMask;
+#ifdef GTAP_DEBUG_IDS
+            if (ld_cg(&A.dbg_live[src(e) & kIdMask]) != 1) GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, src(e) & kIdMask, k, 14, e);
+            const unsigned pos = (b + (unsigned)e) & kPosMask;
+            A.dbg_slotpos[dq_slot_ptr(A, k, S.worker, pos) - A.dq_slots] = pos;
+#endif
+        }
+#ifdef GTAP_DEBUG_IDS
+        if (lane == 0) {
+            unsigned long long w = ld_relaxed(dq_ctl_ptr(A, k, S.worker));
+            if (dq_bottom(w) != b) GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, (int)dq_bottom(w), k, 10, (int)b);
+        }
+#endif
+        // every lane orders its own slot and task-record stores before the
+        // publication (one warp-wide fence), then one lane moves the bottom
+        fence_acq_rel();
         __syncwarp();
         if (lane == 0) {
-            red_add_release(dq_ctl_ptr(A, k, S.worker), (unsigned long long)direct << kPosBits);
+            red_add_relaxed(dq_ctl_ptr(A, k, S.worker), (unsigned long long)direct << kPosBits);
             S.bottom[k] = (b + (unsigned)direct) & kPosMask;
             S.st[GTAP_STAT_PUBLISHED] += (unsigned long long)direct;
         }
@@ -500,6 +576,9 @@ __device__ void publish_src(const Arena& A, WarpShared& S, int k, const int* bas
     for (int base = direct; base < m; base += 32) {
         int take = min(32, m - base);
         int id = ((int)lane < take) ? (src(base + (int)lane) & kIdMask) : 0;
+#ifdef GTAP_DEBUG_IDS
+        if ((int)lane < take && ld_cg(&A.dbg_live[id]) != 1) GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, id, k, 16, base);
+#endif
         fence_acq_rel();
         ring_push_warp(A, A.overflow, id, take);
         if (lane == 0) S.st[GTAP_STAT_OVERFLOW_PUSHES] += (unsigned long long)take;
@@ -567,6 +646,12 @@ __device__ int admit(const Arena& A, WarpShared& S, int& my_tid) {
         const gtap_root& rd = A.roots[slot];
         int id = alloc_id(A, S);
         if (id >= A.total_ids) id = A.total_ids;   // error recorded; the launch aborts
+#ifdef GTAP_DEBUG_IDS
+        if (id < A.total_ids) {
+            if (atomicExch(&A.dbg_live[id], 1) != 0) GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, id, -1, 4, 0);
+            atomicExch(&A.dbg_exec[id], 0);
+        }
+#endif
         int kind = Prog::root_kind(rd.kind);
         if (kind < 0) {
             GTAP_ERROR(A, ERR_INVALID_KIND, id, -1, rd.kind, GTAP_KIND_COUNT);
@@ -612,6 +697,7 @@ __device__ void worker_loop(const Arena& A, WarpShared& S) {
     bool having = false;
     const unsigned long long t_start = global_ns();
     int round = 0;
+    int src_kind = 0;                        // debug builds: where this round's tasks came from
     bool idle = false;                       // counted in the hungry replicas
     int* const hungry_mine = A.hungry + (S.worker % kHungryReplicas) * kHungryStride;
     auto hungry_add = [&](int d) {
@@ -633,13 +719,23 @@ __device__ void worker_loop(const Arena& A, WarpShared& S) {
             for (int kk = 0; kk < Q && nb == 0; ++kk) {
                 int k = (S.cur_q + kk) % Q;
                 nb = pop_own(A, S, k, my_tid);
-                if (nb == 0) nb = steal(A, S, k, rng, last_victim, my_tid);
+                src_kind = 1;
+                if (nb == 0) {
+                    nb = steal(A, S, k, rng, last_victim, my_tid);
+                    src_kind = 2;
+                }
                 if (nb) {
                     if (lane == 0) S.cur_q = k;
                 }
             }
-            if (nb == 0) nb = ring_pop_warp(A, A.overflow, 32, &my_tid);
-            if (nb == 0) nb = admit<Prog>(A, S, my_tid);
+            if (nb == 0) {
+                nb = ring_pop_warp(A, A.overflow, 32, &my_tid);
+                src_kind = 3;
+            }
+            if (nb == 0) {
+                nb = admit<Prog>(A, S, my_tid);
+                src_kind = 4;
+            }
             __syncwarp();
             if (nb == 0) {
                 if (having) {
@@ -689,14 +785,21 @@ __device__ void worker_loop(const Arena& A, WarpShared& S) {
             } else {
                 // header and the first 32 frame bytes in one round trip
                 const char* rec = A.records + (size_t)my_tid * A.rec_stride;
-                hw = ld_cg_v4(rec);
-                fw0 = ld_cg_v4(rec + 16);
-                if (A.rec_stride >= 48) fw1 = ld_cg_v4(rec + 32);
+                hw = ld_data_v4(rec);
+                fw0 = ld_data_v4(rec + 16);
+                if (A.rec_stride >= 48) fw1 = ld_data_v4(rec + 32);
                 if ((unsigned)hw.w >= (unsigned)A.n_roots || hw.y < -1 || hw.y >= A.total_ids) bad = 2;
             }
             if (bad) GTAP_ERROR(A, ERR_INVALID_ARGUMENT, my_tid, -1, bad == 1 ? my_tid : hw.w, A.total_ids);
         }
         if (__any_sync(0xffffffffu, bad)) break;   // corrupted id or header: stop this worker, launch aborts
+#ifdef GTAP_DEBUG_IDS
+        if ((int)lane < nb) {
+            if (ld_cg(&A.dbg_live[my_tid]) != 1) GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, my_tid, src_kind, 3, (int)lane * 1000 + nb);
+            int prev = atomicAdd(&A.dbg_exec[my_tid], 1);
+            if ((hw.x & 0xFFFF) == 0 && prev != 0) GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, my_tid, -1, 5, prev);
+        }
+#endif
         if ((int)lane < nb) {
             S.l_tid[lane] = my_tid;
             S.l_w0[lane] = (unsigned)hw.x;
@@ -723,7 +826,7 @@ __device__ void worker_loop(const Arena& A, WarpShared& S) {
                 for (int e = (int)lane; e < n; e += 32) {
                     unsigned ent = (unsigned)sb[e];
                     unsigned sp = ent >> kIdBits;
-                    if ((fin & spawners) >> sp & 1u) st_relaxed(&hdr_of(A, (int)(ent & kIdMask))->parent, -1);
+                    if ((fin & spawners) >> sp & 1u) hdr_of(A, (int)(ent & kIdMask))->parent = -1;
                 }
             }
             __syncwarp();
@@ -742,7 +845,10 @@ __device__ void worker_loop(const Arena& A, WarpShared& S) {
                 }
             }
             // (3) release the finished task's id unless its parent reads its frame
-            if (!((S.retain_mask >> lane) & 1u)) rt_release_id(S, my_tid);
+            if (!((S.retain_mask >> lane) & 1u)) {
+                rt_release_id_dbg(A, my_tid);
+                rt_release_id(S, my_tid);
+            }
         }
         // (4) per-root accounting, one leader per distinct root
         {
@@ -829,7 +935,12 @@ __device__ void worker_loop(const Arena& A, WarpShared& S) {
                 const int size = (int)(hi - lo);
                 const int take = min(32, size);
                 nb_next = take;
-                if ((int)lane < take) next_tid = ls[(hi - (unsigned)take + lane) & (kLocalCap - 1)];
+                if ((int)lane < take) {
+                    next_tid = ls[(hi - (unsigned)take + lane) & (kLocalCap - 1)];
+#ifdef GTAP_DEBUG_IDS
+                    if (ld_cg(&A.dbg_live[next_tid]) != 1) GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, next_tid, kn, 15, take);
+#endif
+                }
                 __syncwarp();
                 if (lane == 0) {
                     S.ls_hi[kn] = hi - (unsigned)take;
@@ -864,6 +975,7 @@ __device__ void worker_loop(const Arena& A, WarpShared& S) {
         nb = nb_next;
         my_tid = next_tid;
         next_tid = -1;
+        src_kind = 0;
         // periodic abort / watchdog check while busy
         if ((++round & 63) == 0) {
             int stop = 0;

@@ -225,6 +225,15 @@ int gtap_gen_rmat(int32_t scale, int32_t edge_factor, uint64_t seed, int32_t* ro
 /* random unbalanced binary tree, 48% left split */
 int gtap_gen_tree(int32_t n, uint64_t seed, int32_t* left, int32_t* right, int32_t* value, int32_t* size);
 
+/* Exactly-once stress test of the scheduler's deques and overflow queue on the
+ * device (NEW, no reference counterpart): every warp publishes unique tokens
+ * through the scheduler's own publish path and consumes them by pop, steal
+ * and overflow-queue reads.  mode selects the consumers that run while tokens
+ * are produced (1 pops, 2 steals, 4 overflow reads; the final drain uses all).
+ * Returns 0 when every produced token was consumed exactly once. */
+int gtap_selftest_queues(int32_t rounds, int32_t per_round_max, int32_t mode, int64_t* produced,
+                         int64_t* consumed, int64_t* duplicates, int64_t* lost);
+
 /* Library version string (NEW). */
 const char* gtap_version(void);
 
