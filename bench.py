@@ -184,7 +184,9 @@ def cpu_baseline(mix, tasks_of, target_s, cores):
     tasks_of(i) gives root i's task count in the GPU formulation."""
     import multiprocessing as mp
     # cost model only decides the sample size; the timing below is measured
-    est = {0: lambda p: 1.6e-9 * 1.618 ** p, 1: lambda p: 4e-9 * 6.0 ** p, 2: lambda p: 9e-8 * p}
+    nq_nodes = {8: 2057, 9: 8394, 10: 35539, 11: 166926}   # search-tree nodes of n-queens(n)
+    est = {0: lambda p: 1.6e-9 * 1.618 ** p, 1: lambda p: 1.2e-8 * nq_nodes.get(p, 6.0 ** p),
+           2: lambda p: 9e-8 * p}
     budget = target_s * cores
     order = np.random.RandomState(7).permutation(mix.n)
     jobs, tasks, spent = [], 0, 0.0

@@ -130,6 +130,7 @@ _SIGS = [
     ("gtap_write_profile", ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p]),
     ("gtap_selftest_queues", ctypes.c_int,
      [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32] + [ctypes.POINTER(ctypes.c_int64)] * 4),
+    ("gtap_get_arena_counters", ctypes.c_int, [ctypes.POINTER(ctypes.c_int64), ctypes.c_int32]),
     ("gtap_gen_keys", ctypes.c_int, [ctypes.c_uint32, ctypes.c_void_p, ctypes.c_int64]),
     ("gtap_gen_mix", ctypes.c_int, [ctypes.c_uint64, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("gtap_gen_rmat", ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p]),
@@ -310,6 +311,13 @@ def serve_shutdown():
     rc = lib().gtap_serve_shutdown(ctypes.byref(st))
     _check(rc, "gtap_serve_shutdown")
     return st
+
+
+def arena_counters():
+    out = (ctypes.c_int64 * 8)()
+    _check(lib().gtap_get_arena_counters(out, 8), "gtap_get_arena_counters")
+    keys = ("fresh_next", "fresh_base", "pool", "overflow_left", "completed", "total_ids", "workers", "status")
+    return dict(zip(keys, list(out)))
 
 
 def selftest_queues(rounds=60, per_round_max=32, mode=7):

@@ -410,7 +410,7 @@ int gtap_default_config(gtap_config* cfg) {
     cfg->steal_batch = 32;
     cfg->victim_policy = GTAP_VICTIM_PROBE_MAX;
     cfg->probe_width = 16;
-    cfg->spawn_capacity = 1024;
+    cfg->spawn_capacity = 512;
     cfg->ids_per_worker = 1024;
     cfg->total_ids = 1 << 26;
     cfg->frame_bytes = BuiltinProgram::kFrameBytes;
@@ -1136,4 +1136,23 @@ extern "C" int gtap_selftest_queues(int32_t rounds, int32_t per_round_max, int32
     int st = read_status();
     if (st) return st;
     return (dups == 0 && hc.bad_tokens == 0 && ones == (long long)hc.produced) ? 0 : GTAP_ERROR_QUEUE_OVERFLOW;
+}
+
+// ---------------------------------------------------------------------------
+// arena counters after the last launch (task-id accounting)
+// ---------------------------------------------------------------------------
+extern "C" int gtap_get_arena_counters(int64_t* out, int32_t n) {
+    if (!out || n < 8) return GTAP_ERROR_INVALID_ARGUMENT;
+    if (!g.initialized) return GTAP_ERROR_NOT_INITIALIZED;
+    unsigned h[kCtrCount];
+    GT_CUDA(cudaMemcpy(h, g.counters, sizeof(h), cudaMemcpyDeviceToHost));
+    out[0] = h[kCtrFresh];                                  // next never-used id
+    out[1] = (long long)g.last_workers * g.cfg.ids_per_worker;   // first id outside the private ranges
+    out[2] = (int64_t)(h[kCtrPoolTail] - h[kCtrPoolHead]);  // recycled ids waiting in the pool
+    out[3] = (int64_t)(h[kCtrOvTail] - h[kCtrOvHead]);      // tasks left in the overflow queue
+    out[4] = h[kCtrCompleted];
+    out[5] = g.cfg.total_ids;
+    out[6] = g.last_workers;
+    out[7] = h[kCtrStatus];
+    return 0;
 }

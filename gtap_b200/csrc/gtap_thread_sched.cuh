@@ -33,9 +33,8 @@
 
 namespace gtap {
 
-constexpr int kAvailCap = 128;
-constexpr int kAvailLow = 48;
-constexpr int kAvailHigh = 96;
+constexpr int kAvailCap = 256;    // per-warp cache of free task ids
+constexpr int kAvailHigh = 240;   // above this, 32 ids go back to the recycled pool
 constexpr int kFreedCap = 96;
 constexpr int kRootBalCap = 8;
 constexpr int kBalChunk = 1024;
@@ -68,6 +67,7 @@ struct WarpShared {
     unsigned top_cache[kMaxQueues];
     int cur_q;                 // EPAQ queue to try first (reference ctx->queue_idx)
     int avail_n, alloc_pos, freed_n, bump;
+    int alloc_last;            // ids this warp allocated last round (refill target)
     int avail[kAvailCap];
     int freed[kFreedCap];
     int nbal;
@@ -92,9 +92,8 @@ struct TaskCtxT {
 __device__ __noinline__ int alloc_id_slow(const Arena& A, WarpShared& S) {
     int b = atomicAdd(&S.bump, 1);
     if (b < A.ids_per_worker) return S.worker * A.ids_per_worker + b;
-    unsigned f = atom_add_relaxed(A.fresh_next, 1u);
-    if (f < (unsigned)A.total_ids) return (int)f;
-    // recycled ids, one at a time (rare: the per-round refill keeps the cache full)
+    // recycled ids before never-used ones, so the arena is only consumed as far
+    // as the live set requires (rare: the per-round refill keeps the cache full)
     const Ring& r = A.idpool;
     const unsigned cap = 1u << r.cap_log2;
     for (int attempt = 0; attempt < 4096; ++attempt) {
@@ -112,6 +111,8 @@ __device__ __noinline__ int alloc_id_slow(const Arena& A, WarpShared& S) {
         }
         __nanosleep(32);
     }
+    unsigned f = atom_add_relaxed(A.fresh_next, 1u);
+    if (f < (unsigned)A.total_ids) return (int)f;
     GTAP_ERROR(A, ERR_POOL_EXHAUSTED, -1, -1, A.total_ids, A.total_ids);
     return A.total_ids;   // the spare record: written to, never staged or run
 }
@@ -130,17 +131,16 @@ __device__ void id_cache_maintain(const Arena& A, WarpShared& S) {
     int consumed = min(S.alloc_pos, S.avail_n);
     int remain = S.avail_n - consumed;
     int nfreed = min(S.freed_n, kFreedCap);
+    const int used_this_round = S.alloc_pos;
     // move remaining entries to the front (read all, then write)
-    int v0 = 0, v1 = 0, v2 = 0, v3 = 0;
-    if ((int)lane < remain) v0 = S.avail[consumed + lane];
-    if ((int)lane + 32 < remain) v1 = S.avail[consumed + lane + 32];
-    if ((int)lane + 64 < remain) v2 = S.avail[consumed + lane + 64];
-    if ((int)lane + 96 < remain) v3 = S.avail[consumed + lane + 96];
+    int v[kAvailCap / 32];
+#pragma unroll
+    for (int j = 0; j < kAvailCap / 32; ++j)
+        v[j] = ((int)lane + 32 * j < remain) ? S.avail[consumed + lane + 32 * j] : 0;
     __syncwarp();
-    if ((int)lane < remain) S.avail[lane] = v0;
-    if ((int)lane + 32 < remain) S.avail[lane + 32] = v1;
-    if ((int)lane + 64 < remain) S.avail[lane + 64] = v2;
-    if ((int)lane + 96 < remain) S.avail[lane + 96] = v3;
+#pragma unroll
+    for (int j = 0; j < kAvailCap / 32; ++j)
+        if ((int)lane + 32 * j < remain) S.avail[lane + 32 * j] = v[j];
     __syncwarp();
     // append freed ids; whatever does not fit goes to the global ring
     int n = remain;
@@ -165,8 +165,9 @@ __device__ void id_cache_maintain(const Arena& A, WarpShared& S) {
         ring_push_warp(A, A.idpool, id, 32);
         n -= 32;
     }
-    // refill
-    if (n < kAvailLow) {
+    // refill to about twice the last round's demand
+    const int target = min(kAvailCap - 32, max(64, 2 * used_this_round));
+    for (int chunk = 0; chunk < 6 && n < target; ++chunk) {
         int got = 0;
         // private range first (no memory traffic)
         int b = S.bump;
@@ -193,12 +194,15 @@ __device__ void id_cache_maintain(const Arena& A, WarpShared& S) {
             }
         }
         n += got;
+        if (got == 0) break;
+        __syncwarp();
     }
     __syncwarp();
     if (lane == 0) {
         S.avail_n = n;
         S.alloc_pos = 0;
         S.freed_n = 0;
+        S.alloc_last = used_this_round;
     }
     __syncwarp();
 }
@@ -235,6 +239,13 @@ __device__ __forceinline__ void* rt_spawn(const Arena& A, WarpShared& S, int kin
     int s = atomicAdd(&S.cnt[q], 1);
     if (s < A.spawn_cap) {
         S.sbuf[q * A.spawn_cap + s] = id | (int)(lane << kIdBits);
+    } else if (detached) {
+        // staging area full: a child that never notifies its parent can go
+        // straight to the global overflow queue (its record is written above)
+        atomicSub(&S.cnt[q], 1);
+        fence_acq_rel();
+        ring_push_one(A.overflow, id);
+        atomicAdd(&S.st[GTAP_STAT_OVERFLOW_PUSHES], 1ull);
     } else {
         GTAP_ERROR(A, ERR_SPAWN_BUFFER_OVERFLOW, S.l_tid[lane], q, s, A.spawn_cap);
     }
@@ -1015,6 +1026,7 @@ __device__ __forceinline__ void thread_worker_body(const Arena& A) {
             S.top_cache[k] = 0;
         }
         S.cur_q = 0;
+        S.alloc_last = 0;
         S.alloc_pos = 0;
         S.freed_n = 0;
         S.nbal = 0;

@@ -234,6 +234,12 @@ int gtap_gen_tree(int32_t n, uint64_t seed, int32_t* left, int32_t* right, int32
 int gtap_selftest_queues(int32_t rounds, int32_t per_round_max, int32_t mode, int64_t* produced,
                          int64_t* consumed, int64_t* duplicates, int64_t* lost);
 
+/* Task-id accounting after the last launch (NEW): out[0] next never-used id,
+ * out[1] first id outside the private per-worker ranges, out[2] recycled ids
+ * in the pool, out[3] tasks left in the overflow queue, out[4] roots
+ * completed, out[5] arena ids, out[6] workers, out[7] status. */
+int gtap_get_arena_counters(int64_t* out, int32_t n);
+
 /* Library version string (NEW). */
 const char* gtap_version(void);
 

@@ -46,10 +46,20 @@ def test_id_pool_exhausted_reports_and_recovers():
 
 
 def test_spawn_buffer_overflow_reports():
+    # cilksort tasks spawn 4 children each that their parent waits for: 32 lanes
+    # stage 128 per round, twice this staging capacity.  (Children nobody waits
+    # for, as in n-queens, spill to the overflow queue instead of failing.)
+    import torch
     gt.gtap_initialize(gt.default_config(spawn_capacity=64))
     try:
-        rc = launch_rc(gt.nq_root(13))
+        n = 1 << 16
+        src = torch.arange(n, 0, -1, dtype=torch.int32, device="cuda")
+        arr = torch.empty_like(src)
+        tmp = torch.empty_like(src)
+        rc = launch_rc(gt.cilksort_root(src.data_ptr(), arr.data_ptr(), tmp.data_ptr(), n))
         assert rc == 7, rc
+        res, st = gt.launch([gt.nq_root(12)])    # detached children: spill, still correct
+        assert res[0].value == 14200
     finally:
         gt.gtap_finalize()
     healthy_afterwards()
