@@ -354,7 +354,7 @@ int launch_resident(int n_roots, cudaStream_t s, float* ms_out, bool light) {
         GT_CUDA(cudaMemsetAsync(g.prof_working, 0, n * sizeof(long long), s));
         GT_CUDA(cudaMemsetAsync(g.prof_tasks, 0, n * sizeof(int), s));
     }
-    ++g.epoch;
+    if ((++g.epoch & 0xFFFFu) == 0) ++g.epoch;   // epoch 0 would match never-written ring slots
 #ifdef GTAP_DEBUG_IDS
     GT_CUDA(cudaMemsetAsync(g.dbg, 0, (size_t)2 * g.cfg.total_ids * sizeof(int), s));
     GT_CUDA(cudaMemsetAsync(g.dbg + 2 * g.cfg.total_ids, 0xFF,
@@ -514,7 +514,7 @@ int gtap_reset(void) {
     if (!g.initialized) return GTAP_ERROR_NOT_INITIALIZED;
     if (g.serving) return GTAP_ERROR_BUSY;
     if (g.h_report) memset(g.h_report, 0, sizeof(GtapErrorReport));
-    ++g.epoch;
+    if ((++g.epoch & 0xFFFFu) == 0) ++g.epoch;   // epoch 0 would match never-written ring slots
     Arena A = make_arena(0, 0, g.workers);
     reset_kernel<<<64, 256>>>(A, g.counters, 0, g.workers * g.cfg.ids_per_worker);
     GT_CUDA(cudaGetLastError());
@@ -775,7 +775,7 @@ extern "C" int gtap_serve_start(int32_t ring_capacity, int32_t admit_watermark) 
     GT_CUDA(cudaEventCreate(&g.serve_ev0));
     GT_CUDA(cudaEventCreate(&g.serve_ev1));
     if (g.h_report) memset(g.h_report, 0, sizeof(GtapErrorReport));
-    ++g.epoch;
+    if ((++g.epoch & 0xFFFFu) == 0) ++g.epoch;   // epoch 0 would match never-written ring slots
     // serve mode runs the light kernel: fib, n-queens, BFS and tree roots
     g.last_workers = g.workers_light;
     Arena A = make_arena(ring_capacity, 2, g.workers_light);
@@ -1110,7 +1110,7 @@ extern "C" int gtap_selftest_queues(int32_t rounds, int32_t per_round_max, int32
     GT_CUDA(cudaMemset(ctr, 0, sizeof(SelftestCounters)));
     GT_CUDA(cudaMalloc(&sums, 2 * sizeof(unsigned long long)));
     GT_CUDA(cudaMemset(sums, 0, 2 * sizeof(unsigned long long)));
-    ++g.epoch;
+    if ((++g.epoch & 0xFFFFu) == 0) ++g.epoch;   // epoch 0 would match never-written ring slots
     Arena A = make_arena(1, 0, W);
     reset_kernel<<<64, 256>>>(A, g.counters, 1, W * g.cfg.ids_per_worker);
     GT_CUDA(cudaGetLastError());

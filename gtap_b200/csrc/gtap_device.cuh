@@ -337,7 +337,7 @@ struct Arena {
 // ---------------------------------------------------------------------------
 // status / errors: first error wins, never trap
 // ---------------------------------------------------------------------------
-__device__ __noinline__ void record_error(const Arena& A, int code, int tid, int queue_idx, int value, int limit,
+static __device__ __noinline__ void record_error(const Arena& A, int code, int tid, int queue_idx, int value, int limit,
                                           int line) {
     if (atomicCAS(A.status, 0, code) == 0) {
         GtapErrorReport* r = A.report;
@@ -368,7 +368,7 @@ __device__ __forceinline__ bool aborted(const Arena& A) { return ld_relaxed(A.ab
 // every task id of the arena, and every value pushed is a distinct live id, so
 // a reservation by atomicAdd can never overrun unconsumed slots.  Values must
 // be published already (the caller issues its release fence before the push).
-__device__ void ring_push_warp(const Arena& A, const Ring& r, int value, int n) {
+static __device__ void ring_push_warp(const Arena& A, const Ring& r, int value, int n) {
     const unsigned lane = lane_id();
     const unsigned cap = 1u << r.cap_log2;
     unsigned pos = 0;
@@ -392,7 +392,7 @@ __device__ __forceinline__ void ring_push_one(const Ring& r, int value) {
 
 // Pop up to `want` values into lanes [0, got).  Slots reserved by a producer
 // but not yet written are waited for with a bounded spin.
-__device__ int ring_pop_warp(const Arena& A, const Ring& r, int want, int* value) {
+static __device__ int ring_pop_warp(const Arena& A, const Ring& r, int want, int* value) {
     const unsigned lane = lane_id();
     const unsigned cap = 1u << r.cap_log2;
     unsigned pos = 0;

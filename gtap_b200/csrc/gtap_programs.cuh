@@ -60,10 +60,29 @@ struct FibFrame {
     int slot;  // byte offset of this task's result in its parent's frame
 };
 
-__device__ __noinline__ int fib_sequential(int n) {
-    // fib_queue_1.cu:9-14: the same doubly recursive work the reference does
-    if (n < 2) return n;
-    return fib_sequential(n - 1) + fib_sequential(n - 2);
+// fib_queue_1.cu:9-14: visits the same call tree as the reference's doubly
+// recursive fib_sequential (every node n >= 2 expands into n-1 and n-2, every
+// leaf adds n), but as a loop: no device stack, so no depth limit from the
+// per-thread stack size.  The walk goes to n-2 first and leaves n-1 pending;
+// pending values along the current path strictly decrease towards the top of
+// the stack, so the stack is a bit set and its top is the lowest set bit.
+// Valid for n <= 64 (roots are checked); the sum wraps like the reference's int.
+static __device__ __noinline__ int fib_sequential(int n) {
+    unsigned long long pending = 0;
+    unsigned sum = 0;
+    int m = n;
+    for (;;) {
+        if (m >= 2) {
+            pending |= 1ull << (m - 1);
+            m -= 2;
+            continue;
+        }
+        sum += (unsigned)m;
+        if (pending == 0) break;
+        m = __ffsll((long long)pending) - 1;
+        pending &= pending - 1;
+    }
+    return (int)sum;
 }
 
 __device__ __forceinline__ void fib_task(const Arena& A, WarpShared& S, void* frame, const int4& w0) {
@@ -117,16 +136,47 @@ struct NqFrame {
     unsigned right;
 };
 
-__device__ __noinline__ int nq_serial(int row, unsigned column, unsigned left, unsigned right, int n) {
-    // gtap_nq.cu:10-23 serial_search, returning the count instead of atomics
-    if (row == n) return 1;
+// gtap_nq.cu:10-23 serial_search, returning the count instead of atomics.
+// The same depth-first search over rows row..n-1, written as a loop so it
+// needs no device stack.  The diagonal masks are kept in 64-bit registers
+// (left unshifted, right shifted up by 32) so that placing a queen can be
+// undone exactly: no bit falls off either end within 32 rows.  Only the
+// column chosen on each row is stored; the candidates still to try on a row
+// are the free columns above that choice (the search takes the lowest first).
+// The last row counts its free columns instead of visiting each one.
+// Valid for 0 <= row <= n <= 32 (roots are checked).
+static __device__ __noinline__ int nq_serial(int row, unsigned column, unsigned left, unsigned right, int n) {
+    if (row >= n) return row == n ? 1 : 0;
     const unsigned mask = (n < 32 ? (1u << n) - 1u : 0xFFFFFFFFu);
-    unsigned avail = mask & ~(column | left | right);
+    unsigned long long L = left, R = (unsigned long long)right << 32;
+    unsigned C = column;
+    unsigned char chosen[32];
+    const int last = n - row - 1;   // depth of the last row below `row`
+    int d = 0;
     int total = 0;
-    while (avail) {
-        unsigned p = avail & (0u - avail);
-        avail -= p;
-        total += nq_serial(row + 1, column | p, (left | p) << 1, (right | p) >> 1, n);
+    unsigned avail = mask & ~(C | (unsigned)L | (unsigned)(R >> 32));
+    for (;;) {
+        if (d == last) {
+            total += __popc(avail);
+            avail = 0;
+        }
+        if (avail) {
+            const unsigned p = avail & (0u - avail);
+            chosen[d] = (unsigned char)(__ffs((int)p) - 1);
+            C |= p;
+            L = (L | p) << 1;
+            R = (R | ((unsigned long long)p << 32)) >> 1;
+            ++d;
+            avail = mask & ~(C | (unsigned)L | (unsigned)(R >> 32));
+            continue;
+        }
+        if (d == 0) break;
+        --d;
+        const unsigned p = 1u << chosen[d];
+        C &= ~p;
+        L = (L >> 1) & ~(unsigned long long)p;
+        R = (R << 1) & ~((unsigned long long)p << 32);
+        avail = mask & ~(C | (unsigned)L | (unsigned)(R >> 32)) & ~((p << 1) - 1u);
     }
     return total;
 }
@@ -173,7 +223,7 @@ struct MergeFrame {
 static_assert(sizeof(SortFrame) <= kFrameBytes && sizeof(MergeFrame) <= kFrameBytes, "frame size");
 
 // cilksort.cu:51-86: 64-element bitonic network in registers, padded with INT_MAX
-__device__ __noinline__ void sort_small(const int* in, int* out, int n) {
+static __device__ __noinline__ void sort_small(const int* in, int* out, int n) {
     int buf[64];
 #pragma unroll
     for (int i = 0; i < 64; ++i) buf[i] = (i < n) ? ld_data(in + i) : 0x7fffffff;
@@ -200,7 +250,7 @@ __device__ __noinline__ void sort_small(const int* in, int* out, int n) {
 }
 
 // cilksort.cu:17-36
-__device__ __noinline__ void merge_seq(const int* a, int alen, const int* b, int blen, int* dst) {
+static __device__ __noinline__ void merge_seq(const int* a, int alen, const int* b, int blen, int* dst) {
     int i = 0, j = 0, k = 0;
     int av = (alen > 0) ? ld_data(a) : 0, bv = (blen > 0) ? ld_data(b) : 0;
     while (i < alen && j < blen) {
@@ -348,7 +398,7 @@ struct MsFrame {
 static_assert(sizeof(MsFrame) <= kFrameBytes, "frame size");
 
 // leaf: <= 64 keys through the register network, <= 128 as two halves + merge
-__device__ __noinline__ void leaf_sort(const int* in, int* out, int* scratch, int n) {
+static __device__ __noinline__ void leaf_sort(const int* in, int* out, int* scratch, int n) {
     if (n <= 64) {
         sort_small(in, out, n);
         return;
@@ -467,22 +517,65 @@ struct TreeFrame {
 };
 static_assert(sizeof(TreeFrame) <= kFrameBytes, "frame size");
 
-__device__ __noinline__ long long tree_serial(const int* left, const int* right, const int* value, int node) {
-    int stack[64];
-    int sp = 0;
+// Sum of the subtree at `node`, whose size is `sz`, without recursion.  A
+// subtree of at most 64 nodes is at most 64 deep, so a plain depth-first walk
+// keeps at most 63 right children pending.  A larger subtree (a cutoff above
+// 64) is walked into its smaller child first with the larger one pending, so
+// each pending entry at least halves the subtree still being walked and at
+// most 31 are pending.  A size array that contradicts the links can still fill
+// the stack, and links with a cycle would walk forever; both set *bad (the
+// walk stops after sz visits) and the sum is wrong, never a fault or a hang.
+static __device__ __noinline__ long long tree_serial(const int* left, const int* right, const int* value,
+                                                     const int* size, int node, int sz, bool* bad) {
     long long total = 0;
-    stack[sp++] = node;
-    while (sp > 0) {
-        const int v = stack[--sp];
+    int budget = sz;
+    if (sz <= 64) {
+        int stack[64];
+        int sp = 0;
+        stack[sp++] = node;
+        while (sp > 0) {
+            if (--budget < 0) { *bad = true; break; }
+            const int v = stack[--sp];
+            total += __ldg(value + v);
+            const int l = __ldg(left + v), r = __ldg(right + v);
+            if (r >= 0) {
+                if (sp < 64) stack[sp++] = r;
+                else *bad = true;
+            }
+            if (l >= 0) {
+                if (sp < 64) stack[sp++] = l;
+                else *bad = true;
+            }
+        }
+        return total;
+    }
+    int pend_node[32], pend_size[32];
+    int sp = 0;
+    int v = node;
+    for (;;) {
+        if (--budget < 0) { *bad = true; break; }
         total += __ldg(value + v);
         const int l = __ldg(left + v), r = __ldg(right + v);
-        if (r >= 0) {
-            if (sp < 64) stack[sp++] = r;
-            else total += tree_serial(left, right, value, r);
-        }
-        if (l >= 0) {
-            if (sp < 64) stack[sp++] = l;
-            else total += tree_serial(left, right, value, l);
+        if (l >= 0 && r >= 0) {
+            const int sl = __ldg(size + l), sr = sz - 1 - sl;
+            const bool left_first = sl <= sr;
+            if (sp < 32) {
+                pend_node[sp] = left_first ? r : l;
+                pend_size[sp] = left_first ? sr : sl;
+                ++sp;
+            } else {
+                *bad = true;
+            }
+            v = left_first ? l : r;
+            sz = left_first ? sl : sr;
+        } else if (l >= 0 || r >= 0) {
+            v = l >= 0 ? l : r;
+            sz -= 1;
+        } else {
+            if (sp == 0) break;
+            --sp;
+            v = pend_node[sp];
+            sz = pend_size[sp];
         }
     }
     return total;
@@ -500,8 +593,11 @@ __device__ __forceinline__ void treesum_task(const Arena& A, WarpShared& S, void
     const int node = w0.x, slot = w0.y;
     switch (rt_state(S)) {
         case 0: {
-            if (__ldg(size + node) <= rd.i1) {
-                return_i64(A, S, slot, tree_serial(left, right, value, node));
+            const int sz = __ldg(size + node);
+            if (sz <= rd.i1) {
+                bool bad = false;
+                return_i64(A, S, slot, tree_serial(left, right, value, size, node, sz, &bad));
+                if (bad) GTAP_ERROR(A, ERR_INVALID_ARGUMENT, S.l_tid[lane_id()], -1, node, sz);
                 rt_finish(S);
                 return;
             }
@@ -556,6 +652,16 @@ struct BuiltinProgramT {
             case GTAP_KIND_BFS: return prog::K_BFS;
             case GTAP_KIND_TREESUM: return prog::K_TREESUM;
             default: return -1;
+        }
+    }
+
+    // Argument ranges the built-in tasks rely on: fib's serial leaf handles
+    // n <= 64, n-queens packs n and the cutoff into 8 bits with n <= 32 columns.
+    __device__ static bool root_args_ok(const gtap_root& rd) {
+        switch (rd.kind) {
+            case GTAP_KIND_FIB: return rd.i0 <= 64;
+            case GTAP_KIND_NQ: return rd.i0 >= 0 && rd.i0 <= 32 && rd.i1 >= 0 && rd.i1 < 256;
+            default: return true;
         }
     }
 

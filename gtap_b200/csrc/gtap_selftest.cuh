@@ -23,7 +23,7 @@ struct SelftestCounters {
 
 // mode bits select the consumers active while tokens are produced:
 // 1 = own-deque pops, 2 = steals, 4 = overflow-queue reads (all run in the drain)
-__global__ void selftest_queue_kernel(const Arena A, int rounds, int per_round_max, unsigned* seen,
+static __global__ void selftest_queue_kernel(const Arena A, int rounds, int per_round_max, unsigned* seen,
                                       SelftestCounters* c, int mode) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int wib = threadIdx.x >> 5;

@@ -89,7 +89,7 @@ struct TaskCtxT {
 // ---------------------------------------------------------------------------
 // task-id allocation
 // ---------------------------------------------------------------------------
-__device__ __noinline__ int alloc_id_slow(const Arena& A, WarpShared& S) {
+static __device__ __noinline__ int alloc_id_slow(const Arena& A, WarpShared& S) {
     int b = atomicAdd(&S.bump, 1);
     if (b < A.ids_per_worker) return S.worker * A.ids_per_worker + b;
     // recycled ids before never-used ones, so the arena is only consumed as far
@@ -125,7 +125,7 @@ __device__ __forceinline__ int alloc_id(const Arena& A, WarpShared& S) {
 
 // Warp-cooperative: compact the cache after a round, return surplus ids to
 // the global ring and refill from the private range / ring / fresh ids.
-__device__ void id_cache_maintain(const Arena& A, WarpShared& S) {
+static __device__ void id_cache_maintain(const Arena& A, WarpShared& S) {
     const unsigned lane = lane_id();
     __syncwarp();
     int consumed = min(S.alloc_pos, S.avail_n);
@@ -305,7 +305,7 @@ __device__ __forceinline__ void rt_release_id(WarpShared& S, int tid) {
 // ---------------------------------------------------------------------------
 // root accounting
 // ---------------------------------------------------------------------------
-__device__ void complete_root(const Arena& A, int r) {
+static __device__ void complete_root(const Arena& A, int r) {
     gtap_root_result* res = &A.results[r];
     res->t_done_ns = global_ns();
     __threadfence();
@@ -330,7 +330,7 @@ __device__ __forceinline__ void outstanding_add(const Arena& A, int r, long long
     if (old + d == 0) complete_root(A, r);
 }
 
-__device__ void flush_bal(const Arena& A, RootBal& e) {
+static __device__ void flush_bal(const Arena& A, RootBal& e) {
     if (e.created) red_add_relaxed(reinterpret_cast<long long*>(&A.results[e.root].tasks), (long long)e.created);
     e.created = 0;
     if (e.bal != 0) outstanding_add(A, e.root, -(long long)e.bal);
@@ -338,13 +338,13 @@ __device__ void flush_bal(const Arena& A, RootBal& e) {
 }
 
 // lane 0 only
-__device__ void flush_all_bal(const Arena& A, WarpShared& S) {
+static __device__ void flush_all_bal(const Arena& A, WarpShared& S) {
     for (int i = 0; i < S.nbal; ++i) flush_bal(A, S.bal[i]);
     S.nbal = 0;
 }
 
 // Called by one leader lane per distinct root, serialised across leaders.
-__device__ void account_root(const Arena& A, WarpShared& S, int r, int created, int finished) {
+static __device__ void account_root(const Arena& A, WarpShared& S, int r, int created, int finished) {
     int idx = -1;
     for (int i = 0; i < S.nbal; ++i)
         if (S.bal[i].root == r) { idx = i; break; }
@@ -372,7 +372,7 @@ __device__ void account_root(const Arena& A, WarpShared& S, int r, int created, 
 }
 
 // lane 0: flush entries not touched this round so completions are seen promptly
-__device__ void age_bal(const Arena& A, WarpShared& S) {
+static __device__ void age_bal(const Arena& A, WarpShared& S) {
     int j = 0;
     for (int i = 0; i < S.nbal; ++i) {
         if (S.bal[i].touched) {
@@ -390,7 +390,7 @@ __device__ void age_bal(const Arena& A, WarpShared& S) {
 // deque operations
 // ---------------------------------------------------------------------------
 // Owner pop: LIFO, up to 32 newest published tasks of queue k.
-__device__ int pop_own(const Arena& A, WarpShared& S, int k, int& my_tid) {
+static __device__ int pop_own(const Arena& A, WarpShared& S, int k, int& my_tid) {
     const unsigned lane = lane_id();
     if (((S.bottom[k] - S.top_cache[k]) & kPosMask) == 0) return 0;  // top only grows: surely empty
     int got = 0;
@@ -446,7 +446,7 @@ __device__ __forceinline__ unsigned xorshift32(unsigned& s) {
 // Thief: probe up to probe_width random victims in parallel (one lane each),
 // take up to steal_batch (at most half) of the fullest one's queue k with one
 // CAS on its control word.
-__device__ int steal(const Arena& A, WarpShared& S, int k, unsigned& rng, int& last_victim, int& my_tid) {
+static __device__ int steal(const Arena& A, WarpShared& S, int k, unsigned& rng, int& last_victim, int& my_tid) {
     const unsigned lane = lane_id();
     const int W = A.num_workers;
     if (W < 2) return 0;
@@ -530,7 +530,7 @@ __device__ int steal(const Arena& A, WarpShared& S, int k, unsigned& rng, int& l
 // Publish m entries src[(start + i) & mask] to this warp's deque of queue k
 // (thieves see them after the release add), spilling to the overflow queue
 // when the deque is full.
-__device__ void publish_src(const Arena& A, WarpShared& S, int k, const int* base, unsigned start, unsigned mask,
+static __device__ void publish_src(const Arena& A, WarpShared& S, int k, const int* base, unsigned start, unsigned mask,
                             int m) {
     const unsigned lane = lane_id();
     const unsigned cap = 1u << A.deque_cap_log2;
@@ -619,7 +619,7 @@ __device__ __forceinline__ void prof_working(const Arena& A, WarpShared& S, int 
 // admission: claim roots from the root table (batch) or the published ring (serve)
 // ---------------------------------------------------------------------------
 template <class Prog>
-__device__ int admit(const Arena& A, WarpShared& S, int& my_tid) {
+static __device__ int admit(const Arena& A, WarpShared& S, int& my_tid) {
     const unsigned lane = lane_id();
     int first = 0, k = 0;
     if (lane == 0) {
@@ -667,6 +667,9 @@ __device__ int admit(const Arena& A, WarpShared& S, int& my_tid) {
         if (kind < 0) {
             GTAP_ERROR(A, ERR_INVALID_KIND, id, -1, rd.kind, GTAP_KIND_COUNT);
             kind = 0;
+        } else if (!Prog::root_args_ok(rd)) {
+            GTAP_ERROR(A, ERR_INVALID_ARGUMENT, id, -1, rd.kind, 0);
+            kind = 0;
         }
         TaskHeader* h = hdr_of(A, id);
         int4 hw;
@@ -697,7 +700,7 @@ __device__ int admit(const Arena& A, WarpShared& S, int& my_tid) {
 // the persistent worker loop
 // ---------------------------------------------------------------------------
 template <class Prog>
-__device__ void worker_loop(const Arena& A, WarpShared& S) {
+static __device__ void worker_loop(const Arena& A, WarpShared& S) {
     const unsigned lane = lane_id();
     int my_tid = -1;
     int nb = 0;

@@ -98,12 +98,13 @@ typedef struct gtap_config {
 /* built-in task kinds and root descriptors (NEW)                           */
 /* ------------------------------------------------------------------------ */
 enum {
-    GTAP_KIND_FIB = 1,        /* i0 = n, i1 = sequential cutoff (n < i1 runs serially); value = fib(n) */
-    GTAP_KIND_NQ = 2,         /* i0 = n, i1 = cutoff depth (rows <= i1 fork); value = solutions */
+    GTAP_KIND_FIB = 1,        /* i0 = n (<= 64), i1 = sequential cutoff (n < i1 runs serially); value = fib(n) */
+    GTAP_KIND_NQ = 2,         /* i0 = n (0..32), i1 = cutoff depth (0..255; rows <= i1 fork); value = solutions */
     GTAP_KIND_CILKSORT = 3,   /* p0 = src, p1 = arr (sorted out), p2 = tmp, n = keys, i0 = sort cutoff, i1 = merge cutoff */
     GTAP_KIND_MERGESORT = 4,  /* p0 = src, p1 = arr (sorted out), p2 = tmp, n = keys, i0 = cutoff */
     GTAP_KIND_BFS = 5,        /* p0 = row offsets, p1 = columns, p2 = depth (in/out), i0 = source, i1 = split threshold */
-    GTAP_KIND_TREESUM = 6,    /* p0 = left, p1 = right, p2 = value, i0 = root node, i1 = serial cutoff depth; value = sum */
+    GTAP_KIND_TREESUM = 6,    /* p0 = left, p1 = right, p2 = value, p3 = subtree sizes, i0 = root node,
+                                 i1 = serial cutoff (subtrees of <= i1 nodes are summed serially); value = sum */
     GTAP_KIND_COUNT
 };
 

@@ -85,3 +85,17 @@ def test_unknown_kind_rejected_on_device():
         assert res[0].value == 610
     finally:
         gt.gtap_finalize()
+
+
+@pytest.mark.parametrize("root", [gt.fib_root(65), gt.nq_root(33), gt.nq_root(8, 256)])
+def test_out_of_range_root_rejected_on_device(root):
+    # fib's serial leaf handles n <= 64; n-queens has at most 32 columns and
+    # packs its cutoff into 8 bits
+    gt.gtap_initialize(gt.default_config())
+    try:
+        rc = launch_rc(root)
+        assert rc == 11, rc   # GTAP_ERROR_INVALID_ARGUMENT
+        res, st = gt.launch([gt.fib_root(15)])
+        assert res[0].value == 610
+    finally:
+        gt.gtap_finalize()

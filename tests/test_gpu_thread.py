@@ -111,6 +111,35 @@ def test_treesum(rt, n, cutoff):
     assert r.value == orc.tree_sum(left, right, value, 0)
 
 
+# Serial leaves deeper than any earlier cutoff: the leaves are loops with a
+# bounded stack of their own, so their depth does not depend on the device's
+# per-thread stack size.
+@pytest.mark.parametrize("n,cutoff", [(30, 31), (32, 20), (33, 16)])
+def test_fib_deep_serial_leaves(rt, n, cutoff):
+    r, st = run1(gt.fib_root(n, cutoff=cutoff))
+    assert r.status == gt.ROOT_DONE
+    assert r.value == orc.fib(n)
+    assert r.tasks == orc.fib_tasks(n, cutoff)
+
+
+@pytest.mark.parametrize("n,cut", [(14, 0), (12, 1), (8, 0)])
+def test_nq_deep_serial_leaves(rt, n, cut):
+    r, st = run1(gt.nq_root(n, cut))
+    assert r.value == orc.nq(n)
+    assert r.tasks == orc.nq_tasks(n, cut)
+
+
+@pytest.mark.parametrize("cutoff", [65, 5000, 1 << 16])
+def test_treesum_large_cutoff(rt, cutoff):
+    # subtrees above 64 nodes take the size-guided walk (smaller child first)
+    n = 1 << 16
+    left, right, value, size = gt.gen_tree(n, 9)
+    d = [dev(x) for x in (left, right, value, size)]
+    r, st = run1(gt.treesum_root(*[dptr(x) for x in d], n, 0, cutoff))
+    assert r.status == gt.ROOT_DONE
+    assert r.value == orc.tree_sum(left, right, value, 0)
+
+
 def mixed_roots(keep):
     import torch
     roots, expect, bufs = [], [], []
