@@ -22,7 +22,7 @@ NVCC_FLAGS = [
 
 
 def sources():
-    return [os.path.join(CSRC, "gtap_capi.cu")]
+    return [os.path.join(CSRC, "gtap_capi.cu"), os.path.join(CSRC, "gtap_noalloc.cu")]
 
 
 def deps():

@@ -201,6 +201,7 @@ Arena make_arena(int n_roots, int mode, int workers) {
     A.probe_width = c.probe_width;
     A.spawn_cap = c.spawn_capacity;
     A.ids_per_worker = c.ids_per_worker;
+    A.avail_target = kAvailCap - 32;
     A.rec_stride = kHdrBytes + ((c.frame_bytes + 15) / 16) * 16;
     A.admit_batch = c.admit_batch;
     A.mode = mode;

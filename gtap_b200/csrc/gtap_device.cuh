@@ -267,6 +267,7 @@ struct Arena {
     int probe_width;        // victims probed per steal attempt (thread mode)
     int spawn_cap;          // staged children per queue per worker and round
     int ids_per_worker;     // private initial id range per worker
+    int avail_target;       // most free ids a worker keeps cached (<= 224)
     int rec_stride;         // bytes per task record
     int admit_batch;        // roots claimed per admission
     int mode;               // GTAP_MODE_*

@@ -159,14 +159,14 @@ static __device__ void id_cache_maintain(const Arena& A, WarpShared& S) {
         __syncwarp();
     }
     // surplus: give 32 back
-    if (n > kAvailHigh) {
+    if (n > min(kAvailHigh, A.avail_target + 32)) {
         int id = S.avail[n - 32 + lane];
         __syncwarp();
         ring_push_warp(A, A.idpool, id, 32);
         n -= 32;
     }
     // refill to about twice the last round's demand
-    const int target = min(kAvailCap - 32, max(64, 2 * used_this_round));
+    const int target = min(A.avail_target, max(64, 2 * used_this_round));
     for (int chunk = 0; chunk < 6 && n < target; ++chunk) {
         int got = 0;
         // private range first (no memory traffic)

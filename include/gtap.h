@@ -241,6 +241,22 @@ int gtap_selftest_queues(int32_t rounds, int32_t per_round_max, int32_t mode, in
  * completed, out[5] arena ids, out[6] workers, out[7] status. */
 int gtap_get_arena_counters(int64_t* out, int32_t n);
 
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory (a serving loop that must avoid an allocation's implicit device-wide
+ * synchronisation, or a process whose HBM already belongs to another
+ * allocator): runs n_roots roots in one persistent launch with every piece of
+ * scheduler scratch in a fixed file-scope device array of about 45 MiB that
+ * each GPU loading the library keeps until exit.  d_roots and d_results are
+ * device buffers owned by the caller (so are the arrays the roots point to).
+ * Needs no gtap_initialize().  Limits: at most 4096 roots (else
+ * GTAP_ERROR_INVALID_ARGUMENT), fib / n-queens / BFS / tree-sum kinds only,
+ * 2^19 task records shared by live tasks and per-worker free-id caches (a
+ * tree that outgrows them fails with GTAP_ERROR_TASK_ID_POOL_LOW_HEADROOM).
+ * The first call on a device does a one-time set-up: make it before any
+ * stream capture.  Calls share the array: calls that overlap on the GPU race
+ * and must be serialised.  Synchronous; returns the device status. */
+int gtap_launch_noalloc(const gtap_root* d_roots, int32_t n_roots, gtap_root_result* d_results, void* stream);
+
 /* Library version string (NEW). */
 const char* gtap_version(void);
 
