@@ -222,48 +222,108 @@ struct MergeFrame {
 };
 static_assert(sizeof(SortFrame) <= kFrameBytes && sizeof(MergeFrame) <= kFrameBytes, "frame size");
 
-// cilksort.cu:51-86: 64-element bitonic network in registers, padded with INT_MAX
-static __device__ __noinline__ void sort_small(const int* in, int* out, int n) {
-    int buf[64];
-#pragma unroll
-    for (int i = 0; i < 64; ++i) buf[i] = (i < n) ? ld_data(in + i) : 0x7fffffff;
+// ---------------------------------------------------------------------------
+// Warp-cooperative leaves.  A leaf sort (cilksort.cu:51-86 sort_small_device,
+// mergesort.cu:15-32 mergesort_rec_device) or leaf merge (cilksort.cu:17-36
+// seqmerge) does not run in the lane that reached it: the lane marks its task
+// in leaf_mask and returns, and after the round's task bodies the whole warp
+// works through the marked tasks one at a time (warp_leaves below), before any
+// parent is told that they finished.  Keys move as coalesced 128-byte rows,
+// sorting uses shuffles instead of a per-thread register network, and a leaf
+// may have any length.  The output is the same sorted sequence.
+// ---------------------------------------------------------------------------
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+__device__ __forceinline__ void mark_leaf(WarpShared& S) { atomicOr(&S.leaf_mask, 1u << lane_id()); }
+
+// Bitonic sort of the 64 keys held two per lane (key i = r * 32 + lane in
+// v[r]), ascending.
+__device__ __forceinline__ void warp_bitonic64(int& v0, int& v1) {
+    const unsigned lane = lane_id();
 #pragma unroll
     for (int k = 2; k <= 64; k <<= 1) {
 #pragma unroll
         for (int j = k >> 1; j > 0; j >>= 1) {
-#pragma unroll
-            for (int i = 0; i < 64; ++i) {
-                const int ixj = i ^ j;
-                if (ixj > i) {
-                    const bool up = ((i & k) == 0);
-                    const int a = buf[i], b = buf[ixj];
-                    const bool swap = up ? (a > b) : (a < b);
-                    buf[i] = swap ? b : a;
-                    buf[ixj] = swap ? a : b;
+            if (j == 32) {   // k == 64: key lane pairs with key lane + 32, ascending
+                const int lo = min(v0, v1), hi = max(v0, v1);
+                v0 = lo;
+                v1 = hi;
+            } else {
+                const int p0 = __shfl_xor_sync(kFull, v0, j);
+                const int p1 = __shfl_xor_sync(kFull, v1, j);
+                const bool lower = (lane & (unsigned)j) == 0;
+                const bool up0 = (lane & (unsigned)k) == 0;
+                const bool up1 = ((lane + 32u) & (unsigned)k) == 0;
+                v0 = (lower == up0) ? min(v0, p0) : max(v0, p0);
+                v1 = (lower == up1) ? min(v1, p1) : max(v1, p1);
+            }
+        }
+    }
+}
+
+// dst[0, alen + blen) = merge of sorted a and b (a first among equal keys).
+// Each lane produces 8 consecutive outputs per 256-output tile, starting at
+// the merge-path split of its first output.
+static __device__ __noinline__ void warp_merge(const int* a, int alen, const int* b, int blen, int* dst) {
+    const int lane = (int)lane_id();
+    const int total = alen + blen;
+    for (int t0 = 0; t0 < total; t0 += 256) {
+        const int d = t0 + lane * 8;
+        if (d < total) {
+            int lo = max(0, d - blen), hi = min(d, alen);
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (ld_data(a + mid) <= ld_data(b + (d - 1 - mid))) lo = mid + 1;
+                else hi = mid;
+            }
+            int i = lo, j = d - lo;
+            const int m = min(8, total - d);
+            int av = i < alen ? ld_data(a + i) : 0, bv = j < blen ? ld_data(b + j) : 0;
+            for (int e = 0; e < m; ++e) {
+                const bool take_a = j >= blen || (i < alen && av <= bv);
+                if (take_a) {
+                    dst[d + e] = av;
+                    if (++i < alen) av = ld_data(a + i);
+                } else {
+                    dst[d + e] = bv;
+                    if (++j < blen) bv = ld_data(b + j);
                 }
             }
         }
     }
-#pragma unroll
-    for (int i = 0; i < 64; ++i)
-        if (i < n) out[i] = buf[i];
 }
 
-// cilksort.cu:17-36
-static __device__ __noinline__ void merge_seq(const int* a, int alen, const int* b, int blen, int* dst) {
-    int i = 0, j = 0, k = 0;
-    int av = (alen > 0) ? ld_data(a) : 0, bv = (blen > 0) ? ld_data(b) : 0;
-    while (i < alen && j < blen) {
-        if (av < bv) {
-            dst[k++] = av;
-            if (++i < alen) av = ld_data(a + i);
-        } else {
-            dst[k++] = bv;
-            if (++j < blen) bv = ld_data(b + j);
-        }
+// out[0, n) = in[0, n) sorted; scr is n keys of scratch (in may alias out).
+// 64-key runs by warp_bitonic64, then merge passes of doubling width that
+// alternate between scr and out so the last one lands in out.
+static __device__ __noinline__ void warp_sort(const int* in, int* out, int* scr, int n) {
+    const int lane = (int)lane_id();
+    const int runs = (n + 63) >> 6;
+    int passes = 0;
+    for (int w = 1; w < runs; w <<= 1) ++passes;
+    int* from = (passes & 1) ? scr : out;
+    int* to = (passes & 1) ? out : scr;
+    for (int c = 0; c < n; c += 64) {
+        const int m = min(64, n - c);
+        int v0 = lane < m ? ld_data(in + c + lane) : 0x7fffffff;
+        int v1 = lane + 32 < m ? ld_data(in + c + lane + 32) : 0x7fffffff;
+        __syncwarp();   // every key of this run is read before any is written (in may alias out)
+        warp_bitonic64(v0, v1);
+        if (lane < m) from[c + lane] = v0;
+        if (lane + 32 < m) from[c + lane + 32] = v1;
     }
-    while (i < alen) dst[k++] = ld_data(a + i++);
-    while (j < blen) dst[k++] = ld_data(b + j++);
+    for (int width = 64; width < n; width <<= 1) {
+        __syncwarp();
+        for (int s = 0; s < n; s += 2 * width) {
+            const int alen = min(width, n - s);
+            const int blen = min(width, n - s - alen);
+            warp_merge(from + s, alen, from + s + alen, blen, to + s);
+        }
+        int* t = from;
+        from = to;
+        to = t;
+    }
+    __syncwarp();
 }
 
 // cilksort.cu:38-49: largest index with x[idx] <= val
@@ -304,14 +364,9 @@ __device__ __forceinline__ void cilkmerge_task(const Arena& A, WarpShared& S, vo
         const int* t = a; a = b; b = t;
         int tl = alen; alen = blen; blen = tl;
     }
-    if (blen == 0) {
-        for (int i = 0; i < alen; ++i) dst[i] = ld_data(a + i);
-        rt_finish(S);
-        return;
-    }
     const int cutoff = root_of(A, S).i1;
-    if (alen + blen < cutoff) {
-        merge_seq(a, alen, b, blen, dst);
+    if (blen == 0 || alen + blen < cutoff) {   // a copy or a leaf merge: warp_leaves does it
+        mark_leaf(S);
         rt_finish(S);
         return;
     }
@@ -347,8 +402,8 @@ __device__ __forceinline__ void cilksort_task(const Arena& A, WarpShared& S, voi
     switch (rt_state(S)) {
         case 0: {
             const int sort_cutoff = root_of(A, S).i0;
-            if (n < sort_cutoff) {
-                sort_small(src, arr, n);
+            if (n < sort_cutoff) {   // leaf: warp_leaves sorts src into arr, tmp as scratch
+                if (n > 0) mark_leaf(S);
                 rt_finish(S);
                 return;
             }
@@ -397,17 +452,6 @@ struct MsFrame {
 };
 static_assert(sizeof(MsFrame) <= kFrameBytes, "frame size");
 
-// leaf: <= 64 keys through the register network, <= 128 as two halves + merge
-static __device__ __noinline__ void leaf_sort(const int* in, int* out, int* scratch, int n) {
-    if (n <= 64) {
-        sort_small(in, out, n);
-        return;
-    }
-    sort_small(in, scratch, 64);
-    sort_small(in + 64, scratch + 64, n - 64);
-    merge_seq(scratch, 64, scratch + 64, n - 64, out);
-}
-
 __device__ __forceinline__ void mergesort_task(const Arena& A, WarpShared& S, void* frame, const int4& w0,
                                                const int4& w1) {
     (void)frame;
@@ -420,8 +464,8 @@ __device__ __forceinline__ void mergesort_task(const Arena& A, WarpShared& S, vo
     switch (rt_state(S)) {
         case 0: {
             const int cutoff = root_of(A, S).i0;
-            if (n <= cutoff || n <= 1) {
-                if (n > 0) leaf_sort(in, out, tmp, n);
+            if (n <= cutoff || n <= 1) {   // leaf: warp_leaves sorts in into out, tmp as scratch
+                if (n > 0) mark_leaf(S);
                 rt_finish(S);
                 return;
             }
@@ -704,6 +748,40 @@ struct BuiltinProgramT {
                 break;
             default:
                 break;
+        }
+    }
+
+    // Leaf work of the lanes in `mask`, done by the whole warp: each marked
+    // lane's task kind and frame words (loaded with its header this round)
+    // are broadcast, and the warp sorts or merges for that task.
+    __device__ static void warp_leaves(const Arena& A, WarpShared& S, unsigned mask, int kind, const int4& w0,
+                                       const int4& w1) {
+        (void)A;
+        (void)S;
+        if constexpr (kSorts) {
+        while (mask) {
+            const int l = __ffs(mask) - 1;
+            mask &= mask - 1;
+            const int k = __shfl_sync(prog::kFull, kind, l);
+            const unsigned x0 = (unsigned)__shfl_sync(prog::kFull, w0.x, l), y0 = (unsigned)__shfl_sync(prog::kFull, w0.y, l);
+            const unsigned z0 = (unsigned)__shfl_sync(prog::kFull, w0.z, l), q0 = (unsigned)__shfl_sync(prog::kFull, w0.w, l);
+            const unsigned x1 = (unsigned)__shfl_sync(prog::kFull, w1.x, l), y1 = (unsigned)__shfl_sync(prog::kFull, w1.y, l);
+            const int z1 = __shfl_sync(prog::kFull, w1.z, l), q1 = __shfl_sync(prog::kFull, w1.w, l);
+            int* p0 = reinterpret_cast<int*>((unsigned long long)x0 | ((unsigned long long)y0 << 32));
+            int* p1 = reinterpret_cast<int*>((unsigned long long)z0 | ((unsigned long long)q0 << 32));
+            int* p2 = reinterpret_cast<int*>((unsigned long long)x1 | ((unsigned long long)y1 << 32));
+            switch (k) {
+                case prog::K_CILKSORT: prog::warp_sort(p2, p0, p1, z1); break;   // src -> arr, tmp scratch
+                case prog::K_CILKMERGE: prog::warp_merge(p0, z1, p1, q1, p2); break;   // a, b -> dst
+                case prog::K_MERGESORT: prog::warp_sort(p0, p1, p2, z1); break;   // in -> out, tmp scratch
+                default: break;
+            }
+        }
+        } else {
+            (void)mask;
+            (void)kind;
+            (void)w0;
+            (void)w1;
         }
     }
 

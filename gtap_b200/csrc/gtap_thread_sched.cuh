@@ -62,6 +62,7 @@ struct WarpShared {
     unsigned fin_mask;         // lanes whose task returned this round
     unsigned retain_mask;      // finished lanes whose id the parent releases
     unsigned spawn_mask;       // lanes that spawned this round
+    unsigned leaf_mask;        // lanes whose task left leaf work for the whole warp
     int cnt[kMaxQueues];       // children staged this round, per queue
     unsigned bottom[kMaxQueues];
     unsigned top_cache[kMaxQueues];
@@ -722,6 +723,7 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S) {
         if (lane == 0) {
             S.fin_mask = 0;
             S.retain_mask = 0;
+            S.leaf_mask = 0;
         }
         S.l_created[lane] = 0;
         __syncwarp();
@@ -824,6 +826,14 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S) {
             Prog::exec(A, S, (int)(((unsigned)hw.x >> 16) & 0xFFu), my_tid, frame_of(A, my_tid), fw0, fw1);
         }
         __syncwarp();
+        // ---- leaf work the round's tasks left for the whole warp ----
+        // (sorted runs and merges; done before any parent learns that the
+        // task finished, and fenced so the parent sees the data)
+        if (S.leaf_mask) {
+            Prog::warp_leaves(A, S, S.leaf_mask, (int)(((unsigned)hw.x >> 16) & 0xFFu), fw0, fw1);
+            fence_acq_rel();
+            __syncwarp();
+        }
         prof_working(A, S, nb);
 
         // ---- round end ----
@@ -1037,6 +1047,7 @@ __device__ __forceinline__ void thread_worker_body(const Arena& A) {
         S.prof_w = 0;
         S.fin_mask = 0;
         S.retain_mask = 0;
+        S.leaf_mask = 0;
         for (int i = 0; i < GTAP_STAT_COUNT; ++i) S.st[i] = 0;
     }
     // first ids come from the private range

@@ -92,6 +92,48 @@ def test_mergesort_thread(rt, n):
     assert np.array_equal(out.cpu().numpy(), np.sort(keys))
 
 
+# Leaves of any length: sort cutoffs beyond one 64-key run and merge cutoffs
+# beyond one 256-output tile go through the warp's run-and-merge passes.
+@pytest.mark.parametrize("n,sc,mc", [(1 << 16, 2048, 2048), (100003, 1000, 700), (5000, 6000, 6000),
+                                     ((1 << 20) + 1, 129, 257)])
+def test_cilksort_large_leaves(rt, n, sc, mc):
+    import torch
+    keys = orc.keys(7, n)
+    src = dev(keys)
+    arr = torch.empty_like(src)
+    tmp = torch.empty_like(src)
+    r, st = run1(gt.cilksort_root(dptr(src), dptr(arr), dptr(tmp), n, sc, mc))
+    assert r.status == gt.ROOT_DONE
+    assert np.array_equal(arr.cpu().numpy(), np.sort(keys))
+    _, sort_tasks, merge_tasks = orc.cilksort(keys, sc, mc)
+    assert r.tasks == sort_tasks + merge_tasks
+
+
+@pytest.mark.parametrize("n,cutoff", [(1 << 16, 1000), (77777, 4096), (300, 300)])
+def test_mergesort_large_leaves(rt, n, cutoff):
+    import torch
+    keys = orc.keys(11, n)
+    src = dev(keys)
+    out = torch.empty_like(src)
+    tmp = torch.empty_like(src)
+    r, st = run1(gt.mergesort_root(dptr(src), dptr(out), dptr(tmp), n, cutoff, 256))
+    assert r.status == gt.ROOT_DONE
+    assert np.array_equal(out.cpu().numpy(), np.sort(keys))
+
+
+def test_cilksort_duplicate_heavy_keys(rt):
+    import torch
+    rng = np.random.default_rng(3)
+    keys = rng.integers(-3, 4, size=(1 << 18) + 5).astype(np.int32)
+    keys[::97] = np.iinfo(np.int32).max
+    keys[::89] = np.iinfo(np.int32).min
+    src = dev(keys)
+    arr = torch.empty_like(src)
+    tmp = torch.empty_like(src)
+    r, st = run1(gt.cilksort_root(dptr(src), dptr(arr), dptr(tmp), len(keys), 64, 256))
+    assert np.array_equal(arr.cpu().numpy(), np.sort(keys))
+
+
 @pytest.mark.parametrize("scale", [8, 12, 16])
 def test_bfs_rmat(rt, scale):
     import torch
