@@ -27,11 +27,12 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from gtap_b200.workloads import MERGE_CUTOFF, MIX_SEED, N_ROOTS, SORT_CUTOFF, Mix  # noqa: E402
+from gtap_b200.autotune import load_tuned  # noqa: E402
+
 METRIC = "tasks_per_sec_batched_4096_root_mix"
 UNIT = "tasks/s"
-N_ROOTS = 4096
-MIX_SEED = 42
-SORT_CUTOFF, MERGE_CUTOFF = 64, 256
+TUNED = os.path.join(ROOT, "gtap_b200", "tuned", "b200_mix.json")
 
 # algorithmic bytes per task (frame S written by the parent + read by the child,
 # 8 B deque slot, 8 B join RMW, 4 B result), frame sizes of the lowered tasks
@@ -49,38 +50,9 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-per-root", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--config", default="", help="json dict of gtap_config overrides")
+    ap.add_argument("--config", default="", help="json dict of gtap_config overrides (applied last)")
+    ap.add_argument("--tuned", default=TUNED, help="autotuner result whose overrides are applied first ('' = none)")
     return ap.parse_args()
-
-
-# ---------------------------------------------------------------------------
-# workload
-# ---------------------------------------------------------------------------
-class Mix:
-    def __init__(self, gt, n_roots):
-        self.kind, self.param, self.seed = gt.gen_mix(MIX_SEED, n_roots)
-        sizes = np.where(self.kind == 2, self.param, 0).astype(np.int64)
-        self.offsets = np.concatenate([[0], np.cumsum(sizes)])
-        self.total_keys = int(self.offsets[-1])
-        keys = np.empty(max(self.total_keys, 1), np.int32)
-        for i in np.nonzero(self.kind == 2)[0]:
-            o, n = int(self.offsets[i]), int(self.param[i])
-            keys[o:o + n] = gt.gen_keys(int(self.seed[i]) & 0xFFFFFFFF, n)
-        self.keys = keys
-        self.n = n_roots
-
-    def roots(self, gt, src, arr, tmp, elem=4):
-        rs = []
-        for i in range(self.n):
-            k, p = int(self.kind[i]), int(self.param[i])
-            if k == 0:
-                rs.append(gt.fib_root(p, 0))
-            elif k == 1:
-                rs.append(gt.nq_root(p))
-            else:
-                o = int(self.offsets[i]) * elem
-                rs.append(gt.cilksort_root(src + o, arr + o, tmp + o, p, SORT_CUTOFF, MERGE_CUTOFF))
-        return rs
 
 
 def algorithmic_bytes(mix, results):
@@ -277,7 +249,9 @@ def main():
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     import gtap_b200 as gt
 
-    overrides = json.loads(args.config) if args.config else {}
+    overrides = load_tuned(args.tuned) if args.tuned else {}
+    tuned_from = os.path.relpath(args.tuned, ROOT) if overrides else None
+    overrides.update(json.loads(args.config) if args.config else {})
     cfg = gt.gtap_initialize(gt.default_config(**overrides))
     mix = Mix(gt, args.roots)
     src = torch.from_numpy(mix.keys).cuda()
@@ -367,7 +341,7 @@ def main():
                        "roots": args.roots, "mix_seed": MIX_SEED, "tasks_per_step": tasks_per_step,
                        "l2": "inputs larger than L2 (%.2f GB key slabs)" % (3 * mix.total_keys * 4 / 1e9),
                        "parallelism": "replicas" if world > 1 else "single GPU",
-                       "runtime": {k: v for k, v in cfg.as_dict().items()}},
+                       "runtime": {k: v for k, v in cfg.as_dict().items()}, "tuned_from": tuned_from},
             "verified": verified, "gpu_launches": 2 * args.steps, "e2e": e2e, "roofline": roof,
             "cpu_baseline": cpu, "per_root_launch": per_root, "clocks": ck,
             "scheduler": {"steal_success_rate": counters.get("steal_successes", 0) /

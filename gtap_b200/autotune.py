@@ -1,0 +1,182 @@
+"""Autotuner for the scheduler's launch parameters.
+
+The reference fixes its scheduler geometry at compile time (GTAP_BLOCK_SIZE,
+GRID, GTAP_MAX_TASKS_PER_WARP, GTAP_NUM_QUEUES in
+runtime/detail/common/gtap_config.cuh:6-28); here they are launch-time fields
+of gtap_config, so they can be searched per workload and device.
+
+Search: coordinate descent from the library defaults over
+  block          threads per block (warps per block = block / 32)
+  warps_per_sm   resident workers per SM (grid = warps_per_sm * SMs / warps per block,
+                 capped by the kernel's occupancy)
+  deque_capacity per worker and queue
+  steal_batch    tasks moved by one steal
+  probe_width    victims probed in parallel per steal attempt
+  victim_policy  random / last success / fullest of the probed
+  num_queues     EPAQ queues
+Each trial re-initialises the runtime with the candidate configuration, runs
+one warm-up launch and `reps` timed launches (CUDA events around the
+persistent kernel) and keeps the median.  Every trial's results must equal the
+first trial's (values, task counts of deterministic kinds, statuses), so a
+configuration that breaks a result cannot win.
+
+    python -m gtap_b200.autotune --workload mix --out gtap_b200/tuned/b200_mix.json
+"""
+import argparse
+import json
+import os
+import statistics
+import sys
+import time
+
+SPACE = {
+    "warps_per_sm": [4, 8, 12, 16, 24, 32],
+    "block": [64, 128, 256, 512, 1024],
+    "deque_capacity": [256, 1024, 4096, 8192],
+    "steal_batch": [1, 8, 32],
+    "probe_width": [1, 4, 16, 32],
+    "victim_policy": [0, 1, 2],
+    "num_queues": [1, 2, 4],
+}
+ORDER = ["warps_per_sm", "block", "steal_batch", "deque_capacity", "probe_width", "victim_policy", "num_queues"]
+
+
+def to_overrides(point, sm_count):
+    """Tuner point -> gtap_config field overrides."""
+    o = {k: v for k, v in point.items() if k != "warps_per_sm"}
+    block = point.get("block", 256)
+    wpb = max(1, block // 32)
+    if "warps_per_sm" in point:
+        o["grid"] = max(1, (point["warps_per_sm"] * sm_count) // wpb)
+    return o
+
+
+def coordinate_descent(measure, start, space=SPACE, order=ORDER, sweeps=2, log=None):
+    """Minimise measure(point) -> seconds (or None when the point is invalid)
+    one coordinate at a time.  Returns (best_point, best_time, trials)."""
+    best = dict(start)
+    cache = {}
+
+    def evaluate(p):
+        key = tuple(sorted(p.items()))
+        if key not in cache:
+            cache[key] = measure(p)
+            if log:
+                log(p, cache[key])
+        return cache[key]
+
+    best_t = evaluate(best)
+    if best_t is None:
+        raise ValueError("the starting point is not valid")
+    for _ in range(sweeps):
+        improved = False
+        for name in order:
+            for v in space[name]:
+                if v == best.get(name):
+                    continue
+                cand = dict(best)
+                cand[name] = v
+                t = evaluate(cand)
+                if t is not None and t < best_t:
+                    best, best_t, improved = cand, t, True
+        if not improved:
+            break
+    trials = [{"point": dict(k), "s": v} for k, v in cache.items()]
+    return best, best_t, trials
+
+
+def _signature(gt, res):
+    out = []
+    for r in res:
+        out.append((r.status, r.value, r.tasks))
+    return out
+
+
+def run(workload="mix", reps=3, sweeps=2, n_roots=None, out=None, quiet=False):
+    import torch
+    import gtap_b200 as gt
+    from gtap_b200 import workloads as wl
+
+    torch.cuda.init()
+    sm_count = torch.cuda.get_device_properties(0).multi_processor_count
+    keep = []
+    if workload == "mix":
+        mix = wl.Mix(gt, n_roots or wl.N_ROOTS)
+        src, arr, tmp = mix.device_slabs()
+        keep += [src, arr, tmp]
+        roots = mix.roots(gt, src.data_ptr(), arr.data_ptr(), tmp.data_ptr())
+    else:
+        roots = wl.single_root_workload(gt, workload)
+    # every kind in these workloads has a fixed task tree (cilksort's depends
+    # only on the keys), so values and task counts must not change
+    ref_sig = {}
+
+    def measure(point):
+        over = to_overrides(point, sm_count)
+        try:
+            gt.gtap_initialize(gt.default_config(**over))
+        except gt.GtapError:
+            return None
+        try:
+            res, st = gt.launch(roots)                      # warm-up
+            sig = _signature(gt, res)
+            if "sig" not in ref_sig:
+                ref_sig["sig"] = sig
+            elif sig != ref_sig["sig"]:
+                raise RuntimeError("configuration %s changed a result" % over)
+            ms = []
+            for _ in range(reps):
+                res, st = gt.launch(roots)
+                ms.append(st.kernel_ms)
+            return statistics.median(ms) / 1e3
+        except gt.GtapError:
+            return None
+        finally:
+            gt.gtap_finalize()
+
+    def log(p, t):
+        if not quiet:
+            print("%-110s %s" % (json.dumps(p), "invalid" if t is None else "%.3f ms" % (t * 1e3)), flush=True)
+
+    defaults = gt.default_config()
+    start = {"warps_per_sm": 8, "block": defaults.block, "deque_capacity": defaults.deque_capacity,
+             "steal_batch": defaults.steal_batch, "probe_width": defaults.probe_width,
+             "victim_policy": defaults.victim_policy, "num_queues": defaults.num_queues}
+    t0 = time.time()
+    best, best_t, trials = coordinate_descent(measure, start, sweeps=sweeps, log=log)
+    result = {"workload": workload, "roots": len(roots), "device": torch.cuda.get_device_name(0),
+              "sm_count": sm_count, "best_point": best, "best_overrides": to_overrides(best, sm_count),
+              "best_kernel_ms": best_t * 1e3, "reps": reps, "trials": len(trials),
+              "search_s": time.time() - t0,
+              "table": sorted(({"point": t["point"], "kernel_ms": None if t["s"] is None else t["s"] * 1e3}
+                               for t in trials), key=lambda e: (e["kernel_ms"] is None, e["kernel_ms"] or 0))}
+    if out:
+        os.makedirs(os.path.dirname(os.path.abspath(out)), exist_ok=True)
+        with open(out, "w") as f:
+            json.dump(result, f, indent=1)
+    return result
+
+
+def load_tuned(path):
+    """gtap_config overrides from a tuner result file, or {} if absent."""
+    try:
+        with open(path) as f:
+            return dict(json.load(f)["best_overrides"])
+    except (OSError, KeyError, ValueError):
+        return {}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--workload", default="mix", choices=["mix", "fib30", "fib34c12", "nq13", "nq13c7"])
+    ap.add_argument("--roots", type=int, default=None)
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--sweeps", type=int, default=2)
+    ap.add_argument("--out", default=None)
+    a = ap.parse_args(argv)
+    r = run(a.workload, a.reps, a.sweeps, a.roots, a.out)
+    print(json.dumps({k: r[k] for k in ("workload", "best_point", "best_overrides", "best_kernel_ms", "trials")}))
+
+
+if __name__ == "__main__":
+    sys.exit(main())
