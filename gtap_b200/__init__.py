@@ -132,6 +132,12 @@ _SIGS = [
      [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32] + [ctypes.POINTER(ctypes.c_int64)] * 4),
     ("gtap_get_arena_counters", ctypes.c_int, [ctypes.POINTER(ctypes.c_int64), ctypes.c_int32]),
     ("gtap_launch_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]),
+    # support of the drop-in task-ABI header for caller-launched kernels
+    ("gtap_external_initialize", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    ("gtap_external_prepare", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64]),
+    ("gtap_external_finalize", ctypes.c_int, []),
+    ("gtap_external_error_code", ctypes.c_int, [ctypes.POINTER(ctypes.c_int32)]),
+    ("gtap_external_check", ctypes.c_int, []),
     ("gtap_gen_keys", ctypes.c_int, [ctypes.c_uint32, ctypes.c_void_p, ctypes.c_int64]),
     ("gtap_gen_mix", ctypes.c_int, [ctypes.c_uint64, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("gtap_gen_rmat", ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p]),

@@ -25,6 +25,21 @@ def sources():
     return [os.path.join(CSRC, "gtap_capi.cu"), os.path.join(CSRC, "gtap_noalloc.cu")]
 
 
+LOWERED = os.path.join(ROOT, "tests", "lowered")
+LOWERED_BIN = os.path.join(LOWERED, "bin")
+
+# Programs lowered to the reference's task ABI, built against the drop-in
+# header include/gtap_thread.cuh: (source, binary, -D settings).  "ref"
+# builds use the reference's own evaluation settings, "b200" builds a
+# geometry for 148 SMs.
+LOWERED_BUILDS = [
+    ("fib_lowered.cu", "fib_ref_geometry",
+     "-DGTAP_GRID_SIZE=4000 -DGTAP_BLOCK_SIZE=32 -DGTAP_MAX_CHILD_TASKS=2"),
+    ("fib_lowered.cu", "fib_b200",
+     "-DGTAP_GRID_SIZE=888 -DGTAP_BLOCK_SIZE=128 -DGTAP_MAX_CHILD_TASKS=2"),
+]
+
+
 def deps():
     out = []
     for d in (CSRC, os.path.join(ROOT, "include")):
@@ -59,5 +74,32 @@ def build(force=False, verbose=False, debug=False):
     return out
 
 
+def build_lowered(force=False, verbose=False):
+    """Compile the lowered programs against include/gtap_thread.cuh, linking
+    libgtap_b200.so (built first).  Returns the binaries' paths."""
+    build(verbose=verbose)
+    os.makedirs(LOWERED_BIN, exist_ok=True)
+    nvcc = os.environ.get("NVCC", "nvcc")
+    header_deps = deps()
+    outs = []
+    for src, name, defs in LOWERED_BUILDS:
+        s = os.path.join(LOWERED, src)
+        out = os.path.join(LOWERED_BIN, name)
+        outs.append(out)
+        if (not force and os.path.exists(out)
+                and all(os.path.getmtime(p) <= os.path.getmtime(out) for p in header_deps + [s, LIB])):
+            continue
+        cmd = ([nvcc, "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
+                "-diag-suppress", "550", "-I", os.path.join(ROOT, "include")] + defs.split()
+               + ["-o", out, s, "-L", HERE, "-lgtap_b200", "-Xlinker", "-rpath", "-Xlinker", "$ORIGIN/../../../gtap_b200"])
+        r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError("nvcc failed building %s" % name)
+    return outs
+
+
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose="-v" in sys.argv, debug="--debug" in sys.argv))
+    if "--lowered" in sys.argv:
+        print("\n".join(build_lowered(force="--force" in sys.argv)))

@@ -20,6 +20,7 @@
 #include <sys/stat.h>
 #include <vector>
 
+#include "../../include/gtap.h"
 #include "gtap_programs.cuh"
 #include "gtap_selftest.cuh"
 
@@ -42,6 +43,7 @@ struct Runtime {
     int workers_full = 0;       // thread_worker_kernel<BuiltinProgram>
     int workers_light = 0;      // thread_worker_kernel_lb<BuiltinProgramLight>
     int last_workers = 0;       // workers of the last launch
+    int external_workers = 0;   // workers of a kernel the caller launches (drop-in header), 0 = none
     int warps_per_block = 0;
     size_t smem_bytes = 0;
     unsigned epoch = 0;
@@ -61,6 +63,7 @@ struct Runtime {
     int* prof_tasks = nullptr;
     gtap_result_handle* handles = nullptr;
     int* handle_meta = nullptr;
+    int* staging = nullptr;                     // caller-launched kernels: per-warp staging buffers
     unsigned overflow_log2 = 20, idpool_log2 = 24;
 
     // roots
@@ -253,6 +256,7 @@ Arena make_arena(int n_roots, int mode, int workers) {
     A.handle_top = reinterpret_cast<int*>(g.counters + kCtrHandleTop);
     A.handle_meta = g.handle_meta;
     A.handle_cap = c.result_handles;
+    A.staging = g.staging;
     return A;
 }
 
@@ -313,6 +317,7 @@ void free_all() {
     F(g.prof_tasks);
     F(g.handles);
     F(g.handle_meta);
+    F(g.staging);
     F(g.d_roots);
     F(g.d_results);
     F(g.d_outstanding);
@@ -324,6 +329,7 @@ void free_all() {
     g_slab_bytes = 0;
     g.d_report = nullptr;
     g.initialized = false;
+    g.external_workers = 0;
 }
 
 int read_status() {
@@ -387,6 +393,21 @@ int launch_resident(int n_roots, cudaStream_t s, float* ms_out, bool light) {
     return read_status();
 }
 
+// The one root of a kernel the caller launches (drop-in header): task id 0,
+// created on the device by __gtap_push_initial_task, counts as admitted.
+__global__ void external_root_kernel(Arena A, unsigned* counters) {
+    A.outstanding[0] = 1;
+    gtap_root_result r;
+    r.value = 0;
+    r.tasks = 1;
+    r.t_admit_ns = global_ns();
+    r.t_done_ns = 0;
+    r.status = GTAP_ROOT_RUNNING;
+    r.index = 0;
+    A.results[0] = r;
+    counters[kCtrNextRoot] = 1;   // nothing left to admit
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -424,8 +445,9 @@ int gtap_default_config(gtap_config* cfg) {
     return 0;
 }
 
-int gtap_initialize(const gtap_config* cfg_in) {
-    std::lock_guard<std::mutex> lk(g_mu);
+// external_workers > 0: the arena also serves a kernel the caller launches
+// with that many warps (the drop-in task-ABI header's exec_kernel).
+static int initialize_impl(const gtap_config* cfg_in, int external_workers) {
     if (g.serving) return GTAP_ERROR_BUSY;
     if (g.initialized) free_all();
     gtap_config c;
@@ -452,12 +474,13 @@ int gtap_initialize(const gtap_config* cfg_in) {
     g.warps_per_block = c.block / 32;
     g.workers_light = grid_light * g.warps_per_block;
     g.workers_full = grid_full * g.warps_per_block;
-    g.workers = std::max(g.workers_light, g.workers_full);
+    g.workers = std::max(std::max(g.workers_light, g.workers_full), external_workers);
+    g.external_workers = external_workers;
     g.last_workers = g.workers_light;
     if (c.grid == 0) c.grid = std::max(grid_light, grid_full);
-    if ((long long)g.workers * c.ids_per_worker > c.total_ids) {
-        // private ranges may use at most half of the arena
-        c.ids_per_worker = (int)(c.total_ids / g.workers / 2);
+    if ((long long)g.workers * c.ids_per_worker + 1 > c.total_ids / 2) {
+        // private ranges may use at most half of the arena (id 0 may be reserved)
+        c.ids_per_worker = (int)((c.total_ids / 2 - 1) / g.workers);
         if (c.ids_per_worker < 64) return GTAP_ERROR_INVALID_ARGUMENT;
     }
     g.cfg = c;
@@ -490,6 +513,8 @@ int gtap_initialize(const gtap_config* cfg_in) {
     }
     GT_CUDA(cudaMalloc(&g.handles, (size_t)c.result_handles * sizeof(gtap_result_handle)));
     GT_CUDA(cudaMalloc(&g.handle_meta, (size_t)c.total_ids * 3 * sizeof(int)));
+    if (external_workers > 0)
+        GT_CUDA(cudaMalloc(&g.staging, (size_t)external_workers * c.num_queues * (c.spawn_capacity + kLocalCap) * sizeof(int)));
     GT_CUDA(cudaHostAlloc(&g.h_report, sizeof(GtapErrorReport), cudaHostAllocMapped));
     memset(g.h_report, 0, sizeof(GtapErrorReport));
     GT_CUDA(cudaHostGetDevicePointer(&g.d_report, g.h_report, 0));
@@ -499,6 +524,11 @@ int gtap_initialize(const gtap_config* cfg_in) {
     g.initialized = true;
     GT_CUDA(cudaDeviceSynchronize());
     return 0;
+}
+
+int gtap_initialize(const gtap_config* cfg_in) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    return initialize_impl(cfg_in, 0);
 }
 
 int gtap_finalize(void) {
@@ -522,6 +552,48 @@ int gtap_reset(void) {
     GT_CUDA(cudaDeviceSynchronize());
     return 0;
 }
+
+int gtap_external_initialize(const gtap_config* cfg, int32_t workers) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (workers < 1 || !cfg) return GTAP_ERROR_INVALID_ARGUMENT;
+    if (g.serving) return GTAP_ERROR_BUSY;
+    if (g.initialized) free_all();
+    return initialize_impl(cfg, workers);
+}
+
+int gtap_external_prepare(void* arena_out, int64_t arena_bytes) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g.initialized || g.external_workers == 0) return GTAP_ERROR_NOT_INITIALIZED;
+    if (!arena_out || arena_bytes != (int64_t)sizeof(Arena)) return GTAP_ERROR_INVALID_ARGUMENT;
+    if (g.serving) return GTAP_ERROR_BUSY;
+    if (g.h_report) memset(g.h_report, 0, sizeof(GtapErrorReport));
+    if (g.cfg.profile_samples > 0) {
+        size_t n = (size_t)g.workers * g.cfg.profile_samples;
+        GT_CUDA(cudaMemset(g.prof_having, 0, n * sizeof(long long)));
+        GT_CUDA(cudaMemset(g.prof_working, 0, n * sizeof(long long)));
+        GT_CUDA(cudaMemset(g.prof_tasks, 0, n * sizeof(int)));
+    }
+    if ((++g.epoch & 0xFFFFu) == 0) ++g.epoch;   // epoch 0 would match never-written ring slots
+    const int W = g.external_workers;
+    g.last_workers = W;
+    Arena A = make_arena(1, 0, W);
+    A.id_base = 1;   // id 0 is the initial task's (its frame is __gtap_get_task_data(0))
+    A.admit_watermark = 0;
+    reset_kernel<<<64, 256>>>(A, g.counters, 1, 1 + W * g.cfg.ids_per_worker);
+    GT_CUDA(cudaGetLastError());
+    external_root_kernel<<<1, 1>>>(A, g.counters);
+    GT_CUDA(cudaGetLastError());
+    GT_CUDA(cudaDeviceSynchronize());
+    g.have_profile = g.cfg.profile_samples > 0;
+    memcpy(arena_out, &A, sizeof(Arena));
+    return 0;
+}
+
+int gtap_external_finalize(void) { return gtap_finalize(); }
+
+int gtap_external_error_code(int32_t* error_code) { return gtap_get_runtime_error_code(error_code); }
+
+int gtap_external_check(void) { return gtap_check_runtime_error(); }
 
 int gtap_get_config(gtap_config* out) {
     if (!out) return GTAP_ERROR_INVALID_ARGUMENT;

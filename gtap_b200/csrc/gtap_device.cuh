@@ -20,7 +20,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
-#include "../../include/gtap.h"
+#include "../../include/gtap_types.h"
 
 namespace gtap {
 
@@ -127,6 +127,15 @@ __device__ __forceinline__ int4 ld_data_v4(const void* p) {
                  : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p) : "memory");
     return v;
 #endif
+}
+__device__ __forceinline__ unsigned long long ld_data_u64(const unsigned long long* p) {
+    unsigned long long v;
+#if GTAP_RECORD_LOAD == 0
+    asm volatile("ld.global.cg.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+#else
+    asm volatile("ld.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+#endif
+    return v;
 }
 __device__ __forceinline__ int ld_data(const int* p) {
     int v;
@@ -271,6 +280,7 @@ struct Arena {
     int rec_stride;         // bytes per task record
     int admit_batch;        // roots claimed per admission
     int mode;               // GTAP_MODE_*
+    int id_base;            // first id of the private ranges (ids below it are reserved)
     int publish_lazy;       // see gtap_config::publish_lazy
     int max_inflight;       // admitted-but-unfinished roots allowed (0 = unlimited)
     int total_ids;          // ids in the arena
@@ -332,6 +342,10 @@ struct Arena {
     gtap_result_handle* handles;
     int* handle_top;
     int* handle_meta;                  // [total_ids][3]: begin, last, count
+
+    // kernels launched by the caller (drop-in header) whose per-warp staging
+    // buffers do not fit static shared memory: [workers][Q][spawn_cap + kLocalCap]
+    int* staging;
     int handle_cap;
 };
 

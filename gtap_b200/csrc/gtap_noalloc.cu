@@ -42,6 +42,7 @@
 #include <algorithm>
 #include <mutex>
 
+#include "../../include/gtap.h"
 #include "gtap_programs.cuh"
 
 using namespace gtap;

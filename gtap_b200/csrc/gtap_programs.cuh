@@ -686,6 +686,8 @@ __device__ __forceinline__ void treesum_task(const Arena& A, WarpShared& S, void
 template <bool kSorts>
 struct BuiltinProgramT {
     static constexpr int kFrameBytes = prog::kFrameBytes;
+    static constexpr bool kFrameWords = true;    // exec gets the first 32 frame bytes
+    static constexpr bool kFuncTable = false;    // kinds are dispatched by the switch below
 
     __device__ static int root_kind(int k) {
         switch (k) {
@@ -787,8 +789,9 @@ struct BuiltinProgramT {
 
     // w0/w1: the first 32 frame bytes, loaded together with the header
     __device__ static void exec(const Arena& A, WarpShared& S, int kind, int tid, void* frame, const int4& w0,
-                                const int4& w1) {
+                                const int4& w1, unsigned long long fn) {
         (void)tid;
+        (void)fn;
         switch (kind) {
             case prog::K_FIB: prog::fib_task(A, S, frame, w0); break;
             case prog::K_NQ: prog::nq_task(A, S, frame, w0); break;

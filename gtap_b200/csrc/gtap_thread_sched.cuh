@@ -92,7 +92,7 @@ struct TaskCtxT {
 // ---------------------------------------------------------------------------
 static __device__ __noinline__ int alloc_id_slow(const Arena& A, WarpShared& S) {
     int b = atomicAdd(&S.bump, 1);
-    if (b < A.ids_per_worker) return S.worker * A.ids_per_worker + b;
+    if (b < A.ids_per_worker) return A.id_base + S.worker * A.ids_per_worker + b;
     // recycled ids before never-used ones, so the arena is only consumed as far
     // as the live set requires (rare: the per-round refill keeps the cache full)
     const Ring& r = A.idpool;
@@ -174,7 +174,7 @@ static __device__ void id_cache_maintain(const Arena& A, WarpShared& S) {
         int b = S.bump;
         if (b < A.ids_per_worker) {
             int k = min(32, A.ids_per_worker - b);
-            if ((int)lane < k) S.avail[n + lane] = S.worker * A.ids_per_worker + b + lane;
+            if ((int)lane < k) S.avail[n + lane] = A.id_base + S.worker * A.ids_per_worker + b + lane;
             got = k;
             __syncwarp();
             if (lane == 0) S.bump = b + k;
@@ -701,10 +701,10 @@ static __device__ int admit(const Arena& A, WarpShared& S, int& my_tid) {
 // the persistent worker loop
 // ---------------------------------------------------------------------------
 template <class Prog>
-static __device__ void worker_loop(const Arena& A, WarpShared& S) {
+static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_tid) {
     const unsigned lane = lane_id();
-    int my_tid = -1;
-    int nb = 0;
+    int my_tid = (initial_tid >= 0 && lane == 0) ? initial_tid : -1;
+    int nb = initial_tid >= 0 ? 1 : 0;
     unsigned rng = 0x9E3779B9u ^ (unsigned)(S.worker * 2654435761u) ^ (lane * 0x85EBCA6Bu) ^ (unsigned)clock64();
     if (rng == 0) rng = 1;
     int last_victim = -1;
@@ -794,16 +794,21 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S) {
         if (lane == 0 && A.publish_lazy) hv = ld_relaxed(hungry_mine);   // consumed at round end
         prof_working(A, S, nb);
         int4 hw = make_int4(0, -1, 0, 0), fw0 = make_int4(0, 0, 0, 0), fw1 = fw0;
+        unsigned long long fn = 0;
         int bad = 0;
         if ((int)lane < nb) {
             if ((unsigned)my_tid >= (unsigned)A.total_ids) {
                 bad = 1;
             } else {
-                // header and the first 32 frame bytes in one round trip
+                // header, the first 32 frame bytes and (programs that call
+                // through a function table) the task function, in one round trip
                 const char* rec = A.records + (size_t)my_tid * A.rec_stride;
                 hw = ld_data_v4(rec);
-                fw0 = ld_data_v4(rec + 16);
-                if (A.rec_stride >= 48) fw1 = ld_data_v4(rec + 32);
+                if (Prog::kFrameWords) {
+                    fw0 = ld_data_v4(rec + 16);
+                    if (A.rec_stride >= 48) fw1 = ld_data_v4(rec + 32);
+                }
+                if (Prog::kFuncTable) fn = ld_data_u64(reinterpret_cast<const unsigned long long*>(A.funcs) + my_tid);
                 if ((unsigned)hw.w >= (unsigned)A.n_roots || hw.y < -1 || hw.y >= A.total_ids) bad = 2;
             }
             if (bad) GTAP_ERROR(A, ERR_INVALID_ARGUMENT, my_tid, -1, bad == 1 ? my_tid : hw.w, A.total_ids);
@@ -823,7 +828,7 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S) {
             S.l_root[lane] = hw.w;
             S.l_spawned[lane] = 0;
             S.l_value[lane] = 0;
-            Prog::exec(A, S, (int)(((unsigned)hw.x >> 16) & 0xFFu), my_tid, frame_of(A, my_tid), fw0, fw1);
+            Prog::exec(A, S, (int)(((unsigned)hw.x >> 16) & 0xFFu), my_tid, frame_of(A, my_tid), fw0, fw1, fn);
         }
         __syncwarp();
         // ---- leaf work the round's tasks left for the whole warp ----
@@ -1016,21 +1021,18 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S) {
     if (lane == 0) flush_all_bal(A, S);
 }
 
-// Kernel: warps_per_block WarpShared records + staging buffers in dynamic smem.
+// One worker (warp): set up its WarpShared record S (this warp's staging
+// buffer sbuf and local stack lstk given by the caller), run the loop, write
+// its statistics.  initial_tid >= 0 starts lane 0 on that task (a task
+// created before the loop, e.g. by the drop-in __gtap_push_initial_task).
 template <class Prog>
-__device__ __forceinline__ void thread_worker_body(const Arena& A) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int wib = threadIdx.x >> 5;
+__device__ __forceinline__ void thread_worker_run(const Arena& A, WarpShared& S, int worker, int* sbuf, int* lstk,
+                                                  int initial_tid) {
     const unsigned lane = lane_id();
-    WarpShared* ws = reinterpret_cast<WarpShared*>(smem_raw);
-    int* sb_base = reinterpret_cast<int*>(smem_raw + sizeof(WarpShared) * A.warps_per_block);
-    int* ls_base = sb_base + (size_t)A.warps_per_block * A.num_queues * A.spawn_cap;
-    WarpShared& S = ws[wib];
-    const int worker = blockIdx.x * A.warps_per_block + wib;
     if (lane == 0) {
         S.worker = worker;
-        S.sbuf = sb_base + (size_t)wib * A.num_queues * A.spawn_cap;
-        S.lstk = ls_base + (size_t)wib * A.num_queues * kLocalCap;
+        S.sbuf = sbuf;
+        S.lstk = lstk;
         for (int k = 0; k < kMaxQueues; ++k) {
             S.ls_lo[k] = 0;
             S.ls_hi[k] = 0;
@@ -1048,20 +1050,35 @@ __device__ __forceinline__ void thread_worker_body(const Arena& A) {
         S.fin_mask = 0;
         S.retain_mask = 0;
         S.leaf_mask = 0;
+        S.spawn_mask = 0;
         for (int i = 0; i < GTAP_STAT_COUNT; ++i) S.st[i] = 0;
     }
     // first ids come from the private range
     const int first = min(64, A.ids_per_worker);
-    if ((int)lane < first) S.avail[lane] = worker * A.ids_per_worker + (int)lane;
-    if ((int)lane + 32 < first) S.avail[lane + 32] = worker * A.ids_per_worker + (int)lane + 32;
+    const int range = A.id_base + worker * A.ids_per_worker;
+    if ((int)lane < first) S.avail[lane] = range + (int)lane;
+    if ((int)lane + 32 < first) S.avail[lane + 32] = range + (int)lane + 32;
     if (lane == 0) {
         S.avail_n = first;
         S.bump = first;
     }
     __syncwarp();
-    worker_loop<Prog>(A, S);
+    worker_loop<Prog>(A, S, initial_tid);
     __syncwarp();
     if ((int)lane < GTAP_STAT_COUNT) A.stats[(size_t)worker * GTAP_STAT_COUNT + lane] = S.st[lane];
+}
+
+// Kernel body: warps_per_block WarpShared records + staging buffers in dynamic smem.
+template <class Prog>
+__device__ __forceinline__ void thread_worker_body(const Arena& A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int wib = threadIdx.x >> 5;
+    WarpShared* ws = reinterpret_cast<WarpShared*>(smem_raw);
+    int* sb_base = reinterpret_cast<int*>(smem_raw + sizeof(WarpShared) * A.warps_per_block);
+    int* ls_base = sb_base + (size_t)A.warps_per_block * A.num_queues * A.spawn_cap;
+    thread_worker_run<Prog>(A, ws[wib], blockIdx.x * A.warps_per_block + wib,
+                            sb_base + (size_t)wib * A.num_queues * A.spawn_cap,
+                            ls_base + (size_t)wib * A.num_queues * kLocalCap, -1);
 }
 
 
