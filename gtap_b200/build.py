@@ -37,6 +37,14 @@ LOWERED_BUILDS = [
      "-DGTAP_GRID_SIZE=4000 -DGTAP_BLOCK_SIZE=32 -DGTAP_MAX_CHILD_TASKS=2"),
     ("fib_lowered.cu", "fib_b200",
      "-DGTAP_GRID_SIZE=888 -DGTAP_BLOCK_SIZE=128 -DGTAP_MAX_CHILD_TASKS=2"),
+    ("nq_lowered.cu", "nq_ref_geometry",
+     "-DGTAP_GRID_SIZE=2000 -DGTAP_BLOCK_SIZE=32 -DGTAP_MAX_CHILD_TASKS=32 -DGTAP_ASSUME_NO_TASKWAIT"),
+    ("nq_lowered.cu", "nq_b200",
+     "-DGTAP_GRID_SIZE=1184 -DGTAP_BLOCK_SIZE=128 -DGTAP_MAX_CHILD_TASKS=32 -DGTAP_ASSUME_NO_TASKWAIT"),
+    ("cilksort_lowered.cu", "cilksort_ref_geometry",
+     "-DGTAP_GRID_SIZE=2000 -DGTAP_BLOCK_SIZE=32 -DGTAP_MAX_CHILD_TASKS=7"),
+    ("cilksort_lowered.cu", "cilksort_b200",
+     "-DGTAP_GRID_SIZE=592 -DGTAP_BLOCK_SIZE=128 -DGTAP_MAX_CHILD_TASKS=7"),
 ]
 
 

@@ -478,8 +478,9 @@ static int initialize_impl(const gtap_config* cfg_in, int external_workers) {
     g.external_workers = external_workers;
     g.last_workers = g.workers_light;
     if (c.grid == 0) c.grid = std::max(grid_light, grid_full);
-    if ((long long)g.workers * c.ids_per_worker + 1 > c.total_ids / 2) {
-        // private ranges may use at most half of the arena (id 0 may be reserved)
+    if ((long long)g.workers * c.ids_per_worker + 1 > c.total_ids) {
+        // private ranges that would not fit may use at most half of the arena
+        // (id 0 may be reserved for a caller-launched kernel's initial task)
         c.ids_per_worker = (int)((c.total_ids / 2 - 1) / g.workers);
         if (c.ids_per_worker < 64) return GTAP_ERROR_INVALID_ARGUMENT;
     }

@@ -156,6 +156,12 @@ __device__ __forceinline__ int atom_add_acq_rel(int* p, int v) {
     asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
     return old;
 }
+// Acquire only: the caller has issued its own release fence before it.
+__device__ __forceinline__ int atom_add_acquire(int* p, int v) {
+    int old;
+    asm volatile("atom.acquire.gpu.global.add.s32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
 __device__ __forceinline__ int atom_add_relaxed(int* p, int v) {
     int old;
     asm volatile("atom.relaxed.gpu.global.add.s32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");

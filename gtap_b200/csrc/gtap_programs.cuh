@@ -226,7 +226,7 @@ static_assert(sizeof(SortFrame) <= kFrameBytes && sizeof(MergeFrame) <= kFrameBy
 // Warp-cooperative leaves.  A leaf sort (cilksort.cu:51-86 sort_small_device,
 // mergesort.cu:15-32 mergesort_rec_device) or leaf merge (cilksort.cu:17-36
 // seqmerge) does not run in the lane that reached it: the lane marks its task
-// in leaf_mask and returns, and after the round's task bodies the whole warp
+// in its lane flags and returns, and after the round's task bodies the whole warp
 // works through the marked tasks one at a time (warp_leaves below), before any
 // parent is told that they finished.  Keys move as coalesced 128-byte rows,
 // sorting uses shuffles instead of a per-thread register network, and a leaf
@@ -234,7 +234,7 @@ static_assert(sizeof(SortFrame) <= kFrameBytes && sizeof(MergeFrame) <= kFrameBy
 // ---------------------------------------------------------------------------
 constexpr unsigned kFull = 0xFFFFFFFFu;
 
-__device__ __forceinline__ void mark_leaf(WarpShared& S) { atomicOr(&S.leaf_mask, 1u << lane_id()); }
+__device__ __forceinline__ void mark_leaf(WarpShared& S) { S.l_flags[lane_id()] |= kLaneLeaf; }
 
 // Bitonic sort of the 64 keys held two per lane (key i = r * 32 + lane in
 // v[r]), ascending.

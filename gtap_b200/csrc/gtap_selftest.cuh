@@ -37,6 +37,7 @@ static __global__ void selftest_queue_kernel(const Arena A, int rounds, int per_
         S.sbuf = sb_base + (size_t)wib * A.num_queues * A.spawn_cap;
         for (int k = 0; k < kMaxQueues; ++k) {
             S.bottom[k] = 0;
+            S.pend[k] = 0;
             S.top_cache[k] = 0;
             S.cnt[k] = 0;
         }

@@ -33,6 +33,28 @@
 
 namespace gtap {
 
+// Profiling builds (-DGTAP_PHASE_TIMERS): lane 0 adds the clock64 cycles of
+// each scheduler phase to statistics slots 10..15 (acquire, load + task
+// bodies, warp leaves + orphans + staging of children and deque slots, fence
+// + publication + joins + id release + resumed parents, root accounting, id
+// cache).  Off by default: the timers cost a few instructions per phase.
+#ifdef GTAP_PHASE_TIMERS
+// slot 9 (overflow pushes) holds the task-record load latency and slot 7
+// (published) the publication fence in these builds
+#define GTAP_PHASE_MARK(t) long long t = clock64()
+#define GTAP_PHASE_MARK_AFTER(t, dep) \
+    long long t;                      \
+    asm volatile("mov.u64 %0, %%clock64;" : "=l"(t) : "r"(dep) : "memory")
+#define GTAP_PHASE_ADD(slot, t0, t1) \
+    do {                                 \
+        if (lane_id() == 0) S.st[slot] += (unsigned long long)((t1) - (t0)); \
+    } while (0)
+#else
+#define GTAP_PHASE_MARK_AFTER(t, dep) (void)0
+#define GTAP_PHASE_MARK(t) (void)0
+#define GTAP_PHASE_ADD(slot, t0, t1) (void)0
+#endif
+
 constexpr int kAvailCap = 256;    // per-warp cache of free task ids
 constexpr int kAvailHigh = 240;   // above this, 32 ids go back to the recycled pool
 constexpr int kFreedCap = 96;
@@ -42,6 +64,12 @@ constexpr int kLocalCap = 128;     // per-warp, per-queue local ready stack (pow
 constexpr int kReserve = 32;       // ready tasks a warp keeps when others are hungry
 constexpr int kHungryReplicas = 8;  // copies of the hungry-worker count, 128 bytes apart
 constexpr int kHungryStride = 32;
+
+// l_flags bits: each lane writes only its own entry, the round end reads them
+// back with ballots (no shared-memory atomics on one word from 32 lanes)
+constexpr int kLaneFinished = 1;   // the task returned (rt_finish)
+constexpr int kLaneRetain = 2;     // ... and its parent reads its frame, so the parent releases the id
+constexpr int kLaneLeaf = 4;       // the task left leaf work for the whole warp (warp_leaves)
 
 struct RootBal {
     int root;
@@ -59,12 +87,10 @@ struct WarpShared {
     int l_spawned[kWarp];      // children spawned since the last taskwait
     int l_created[kWarp];      // tasks this lane created this round
     int l_value[kWarp];        // contributions to the lane's root value (n-queens counts)
-    unsigned fin_mask;         // lanes whose task returned this round
-    unsigned retain_mask;      // finished lanes whose id the parent releases
-    unsigned spawn_mask;       // lanes that spawned this round
-    unsigned leaf_mask;        // lanes whose task left leaf work for the whole warp
+    int l_flags[kWarp];        // this round, per lane: kLaneFinished | kLaneRetain | kLaneLeaf
     int cnt[kMaxQueues];       // children staged this round, per queue
     unsigned bottom[kMaxQueues];
+    int pend[kMaxQueues];      // deque entries written this round, not yet published (publish_commit)
     unsigned top_cache[kMaxQueues];
     int cur_q;                 // EPAQ queue to try first (reference ctx->queue_idx)
     int avail_n, alloc_pos, freed_n, bump;
@@ -118,8 +144,19 @@ static __device__ __noinline__ int alloc_id_slow(const Arena& A, WarpShared& S) 
     return A.total_ids;   // the spare record: written to, never staged or run
 }
 
+// The lanes of `m` (calling together) add one each to *p with a single
+// shared-memory atomic; returns this lane's old value.
+__device__ __forceinline__ int warp_agg_inc(int* p, unsigned m) {
+    const unsigned lane = lane_id();
+    const int leader = __ffs(m) - 1;
+    int base = 0;
+    if ((int)lane == leader) base = atomicAdd(p, __popc(m));
+    base = __shfl_sync(m, base, leader);
+    return base + __popc(m & ((1u << lane) - 1u));
+}
+
 __device__ __forceinline__ int alloc_id(const Arena& A, WarpShared& S) {
-    int a = atomicAdd(&S.alloc_pos, 1);
+    const int a = warp_agg_inc(&S.alloc_pos, __activemask());
     if (a < S.avail_n) return S.avail[a];
     return alloc_id_slow(A, S);
 }
@@ -237,7 +274,8 @@ __device__ __forceinline__ void* rt_spawn(const Arena& A, WarpShared& S, int kin
     hw.z = 0;
     hw.w = S.l_root[lane];
     *reinterpret_cast<int4*>(h) = hw;
-    int s = atomicAdd(&S.cnt[q], 1);
+    const unsigned m = __activemask();
+    const int s = warp_agg_inc(&S.cnt[q], A.num_queues == 1 ? m : __match_any_sync(m, q));
     if (s < A.spawn_cap) {
         S.sbuf[q * A.spawn_cap + s] = id | (int)(lane << kIdBits);
     } else if (detached) {
@@ -246,7 +284,9 @@ __device__ __forceinline__ void* rt_spawn(const Arena& A, WarpShared& S, int kin
         atomicSub(&S.cnt[q], 1);
         fence_acq_rel();
         ring_push_one(A.overflow, id);
+#ifndef GTAP_PHASE_TIMERS
         atomicAdd(&S.st[GTAP_STAT_OVERFLOW_PUSHES], 1ull);
+#endif
     } else {
         GTAP_ERROR(A, ERR_SPAWN_BUFFER_OVERFLOW, S.l_tid[lane], q, s, A.spawn_cap);
     }
@@ -283,9 +323,8 @@ __device__ __forceinline__ bool rt_join(const Arena& A, WarpShared& S, int child
 __device__ __forceinline__ void rt_finish(const WarpShared& S_, bool retain_override = false) {
     WarpShared& S = const_cast<WarpShared&>(S_);
     const unsigned lane = lane_id();
-    atomicOr(&S.fin_mask, 1u << lane);
-    unsigned flags = S.l_w0[lane] >> 24;
-    if ((flags & kFlagRetain) || retain_override) atomicOr(&S.retain_mask, 1u << lane);
+    const unsigned flags = S.l_w0[lane] >> 24;
+    S.l_flags[lane] |= kLaneFinished | (((flags & kFlagRetain) || retain_override) ? kLaneRetain : 0);
 }
 
 __device__ __forceinline__ void rt_release_id_dbg(const Arena& A, int tid) {
@@ -298,7 +337,7 @@ __device__ __forceinline__ void rt_release_id_dbg(const Arena& A, int tid) {
 }
 
 __device__ __forceinline__ void rt_release_id(WarpShared& S, int tid) {
-    int f = atomicAdd(&S.freed_n, 1);
+    const int f = warp_agg_inc(&S.freed_n, __activemask());
     if (f < kFreedCap) S.freed[f] = tid;
     // an overfull freed list loses the id until the next launch resets the arena
 }
@@ -528,11 +567,11 @@ static __device__ int steal(const Arena& A, WarpShared& S, int k, unsigned& rng,
     return 0;
 }
 
-// Publish m entries src[(start + i) & mask] to this warp's deque of queue k
-// (thieves see them after the release add), spilling to the overflow queue
-// when the deque is full.
-static __device__ void publish_src(const Arena& A, WarpShared& S, int k, const int* base, unsigned start, unsigned mask,
-                            int m) {
+// Write m entries src[(start + i) & mask] into this warp's deque of queue k
+// (the owner's bottom moves at once; thieves see them only after
+// publish_commit), spilling to the overflow queue when the deque is full.
+static __device__ void publish_stage(const Arena& A, WarpShared& S, int k, const int* base, unsigned start,
+                                     unsigned mask, int m) {
     const unsigned lane = lane_id();
     const unsigned cap = 1u << A.deque_cap_log2;
     auto src = [&](int i) { return base[(start + (unsigned)i) & mask]; };
@@ -555,7 +594,8 @@ static __device__ void publish_src(const Arena& A, WarpShared& S, int k, const i
 #ifdef GTAP_QUEUE_CHECKS
         if (lane == 0) {
             unsigned long long w = ld_relaxed(dq_ctl_ptr(A, k, S.worker));
-            if (dq_bottom(w) != b) GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, (int)dq_bottom(w), k, 21, (int)b);
+            if (((dq_bottom(w) + (unsigned)S.pend[k]) & kPosMask) != b)
+                GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, (int)dq_bottom(w), k, 21, (int)b);
             if (((b - dq_top(w)) & kPosMask) + (unsigned)direct > cap)
                 GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, (int)dq_top(w), k, 24, (int)S.top_cache[k]);
         }
@@ -568,34 +608,59 @@ static __device__ void publish_src(const Arena& A, WarpShared& S, int k, const i
             A.dbg_slotpos[dq_slot_ptr(A, k, S.worker, pos) - A.dq_slots] = pos;
 #endif
         }
-#ifdef GTAP_DEBUG_IDS
-        if (lane == 0) {
-            unsigned long long w = ld_relaxed(dq_ctl_ptr(A, k, S.worker));
-            if (dq_bottom(w) != b) GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, (int)dq_bottom(w), k, 10, (int)b);
-        }
-#endif
-        // every lane orders its own slot and task-record stores before the
-        // publication (one warp-wide fence), then one lane moves the bottom
-        fence_acq_rel();
         __syncwarp();
         if (lane == 0) {
-            red_add_relaxed(dq_ctl_ptr(A, k, S.worker), (unsigned long long)direct << kPosBits);
             S.bottom[k] = (b + (unsigned)direct) & kPosMask;
-            S.st[GTAP_STAT_PUBLISHED] += (unsigned long long)direct;
+            S.pend[k] += direct;
         }
     }
-    // the rest spills to the global overflow queue
-    for (int base = direct; base < m; base += 32) {
-        int take = min(32, m - base);
-        int id = ((int)lane < take) ? (src(base + (int)lane) & kIdMask) : 0;
+    // the rest spills to the global overflow queue (its own fence: rare)
+    for (int base_i = direct; base_i < m; base_i += 32) {
+        int take = min(32, m - base_i);
+        int id = ((int)lane < take) ? (src(base_i + (int)lane) & kIdMask) : 0;
 #ifdef GTAP_DEBUG_IDS
-        if ((int)lane < take && ld_cg(&A.dbg_live[id]) != 1) GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, id, k, 16, base);
+        if ((int)lane < take && ld_cg(&A.dbg_live[id]) != 1) GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, id, k, 16, base_i);
 #endif
         fence_acq_rel();
         ring_push_warp(A, A.overflow, id, take);
+#ifndef GTAP_PHASE_TIMERS
         if (lane == 0) S.st[GTAP_STAT_OVERFLOW_PUSHES] += (unsigned long long)take;
+#endif
     }
     __syncwarp();
+}
+
+// One warp-wide fence orders every store this warp made so far (task
+// records, results, deque slots) before what follows; then lane 0 moves the
+// bottoms of the deques publish_stage wrote, making those entries stealable.
+// fence: also when nothing is pending (the joins that follow rely on it).
+static __device__ void publish_commit(const Arena& A, WarpShared& S, bool fence) {
+    const unsigned lane = lane_id();
+    bool any = false;
+    for (int k = 0; k < A.num_queues; ++k) any |= S.pend[k] != 0;
+    if (!any && !fence) return;
+    fence_acq_rel();
+    __syncwarp();
+    if (any && lane == 0) {
+        for (int k = 0; k < A.num_queues; ++k) {
+            const int d = S.pend[k];
+            if (d) {
+                red_add_relaxed(dq_ctl_ptr(A, k, S.worker), (unsigned long long)d << kPosBits);
+#ifndef GTAP_PHASE_TIMERS
+                S.st[GTAP_STAT_PUBLISHED] += (unsigned long long)d;
+#endif
+                S.pend[k] = 0;
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// Stage and publish at once.
+static __device__ void publish_src(const Arena& A, WarpShared& S, int k, const int* base, unsigned start,
+                                   unsigned mask, int m) {
+    publish_stage(A, S, k, base, start, mask, m);
+    publish_commit(A, S, false);
 }
 
 // ---------------------------------------------------------------------------
@@ -720,11 +785,8 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
     };
 
     for (;;) {
-        if (lane == 0) {
-            S.fin_mask = 0;
-            S.retain_mask = 0;
-            S.leaf_mask = 0;
-        }
+        GTAP_PHASE_MARK(ph0);
+        S.l_flags[lane] = 0;
         S.l_created[lane] = 0;
         __syncwarp();
 
@@ -789,6 +851,8 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
             }
         }
 
+        GTAP_PHASE_MARK(ph1);
+        GTAP_PHASE_ADD(10, ph0, ph1);
         // ---- execute: lane i runs task my_tid ----
         int hv = 0;
         if (lane == 0 && A.publish_lazy) hv = ld_relaxed(hungry_mine);   // consumed at round end
@@ -814,6 +878,8 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
             if (bad) GTAP_ERROR(A, ERR_INVALID_ARGUMENT, my_tid, -1, bad == 1 ? my_tid : hw.w, A.total_ids);
         }
         if (__any_sync(0xffffffffu, bad)) break;   // corrupted id or header: stop this worker, launch aborts
+        GTAP_PHASE_MARK_AFTER(ph1b, hw.x ^ fw0.x ^ fw1.w ^ (int)fn);
+        GTAP_PHASE_ADD(9, ph1, ph1b);
 #ifdef GTAP_DEBUG_IDS
         if ((int)lane < nb) {
             if (ld_cg(&A.dbg_live[my_tid]) != 1) GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, my_tid, src_kind, 3, (int)lane * 1000 + nb);
@@ -831,11 +897,15 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
             Prog::exec(A, S, (int)(((unsigned)hw.x >> 16) & 0xFFu), my_tid, frame_of(A, my_tid), fw0, fw1, fn);
         }
         __syncwarp();
+        GTAP_PHASE_MARK(ph2);
+        GTAP_PHASE_ADD(11, ph1b, ph2);
         // ---- leaf work the round's tasks left for the whole warp ----
         // (sorted runs and merges; done before any parent learns that the
         // task finished, and fenced so the parent sees the data)
-        if (S.leaf_mask) {
-            Prog::warp_leaves(A, S, S.leaf_mask, (int)(((unsigned)hw.x >> 16) & 0xFFu), fw0, fw1);
+        const int lane_flags = S.l_flags[lane];
+        const unsigned leaves = __ballot_sync(0xffffffffu, (int)lane < nb && (lane_flags & kLaneLeaf));
+        if (leaves) {
+            Prog::warp_leaves(A, S, leaves, (int)(((unsigned)hw.x >> 16) & 0xFFu), fw0, fw1);
             fence_acq_rel();
             __syncwarp();
         }
@@ -843,8 +913,8 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
 
         // ---- round end ----
         int nb_next = 0, next_tid = -1;
-        const unsigned fin = S.fin_mask;
         const bool active = (int)lane < nb;
+        const unsigned fin = __ballot_sync(0xffffffffu, active && (lane_flags & kLaneFinished));
         const bool my_fin = active && ((fin >> lane) & 1u);
         const unsigned spawners = __ballot_sync(0xffffffffu, active && S.l_spawned[lane] > 0);
         // (1) orphans: children of tasks that returned without a taskwait
@@ -860,70 +930,23 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
             }
             __syncwarp();
         }
-        // (2) join: the last child re-enqueues its parent on the resume queue
-        if (my_fin) {
-            const int parent = S.l_parent[lane];
-            if (parent >= 0) {
-                int old = atom_add_acq_rel(&hdr_of(A, parent)->join, -1);
-                if ((old & kJoinCountMask) == 1) {
-                    int q = (old >> 24) & 7;
-                    if (q >= A.num_queues) q = 0;
-                    int s = atomicAdd(&S.cnt[q], 1);
-                    if (s < A.spawn_cap) S.sbuf[q * A.spawn_cap + s] = parent | (int)(lane << kIdBits);
-                    else GTAP_ERROR(A, ERR_SPAWN_BUFFER_OVERFLOW, parent, q, s, A.spawn_cap);
-                }
-            }
-            // (3) release the finished task's id unless its parent reads its frame
-            if (!((S.retain_mask >> lane) & 1u)) {
-                rt_release_id_dbg(A, my_tid);
-                rt_release_id(S, my_tid);
-            }
-        }
-        // (4) per-root accounting, one leader per distinct root
-        {
-            const int created = active ? S.l_created[lane] : 0;
-            const int finished = my_fin ? 1 : 0;
-            const int value = active ? S.l_value[lane] : 0;
-            const int r = active ? S.l_root[lane] : -1;
-            const unsigned amask = __ballot_sync(0xffffffffu, active);
-            unsigned grp = __match_any_sync(0xffffffffu, r);
-            int c_sum = created, f_sum = finished, v_sum = value;
-            if (active) {
-                c_sum = (int)__reduce_add_sync(grp, (unsigned)created);
-                f_sum = (int)__reduce_add_sync(grp, (unsigned)finished);
-                v_sum = (int)__reduce_add_sync(grp, (unsigned)value);
-            }
-            const bool leader = active && ((unsigned)__ffs(grp) - 1u == lane);
-            unsigned leaders = __ballot_sync(0xffffffffu, leader);
-            (void)amask;
-            __syncwarp();
-            while (leaders) {
-                const unsigned l = (unsigned)__ffs(leaders) - 1u;
-                if (lane == l) {
-                    if (v_sum) atomicAdd(reinterpret_cast<unsigned long long*>(&A.results[r].value),
-                                         (unsigned long long)(long long)v_sum);
-                    account_root(A, S, r, c_sum, f_sum);
-                }
-                __syncwarp();
-                leaders &= leaders - 1u;
-            }
-            if (lane == 0) age_bal(A, S);
-            __syncwarp();
-        }
-        // (5) children join their queue's local stack (newest on top); the
-        //     busiest queue's newest <= 32 run next (reference push_batch keeps
-        //     the newest 32 of k_max); the oldest entries become visible to
-        //     thieves only when a stack overflows or some worker is hungry.
+        // (2) this round's children join their queue's local stack (newest on
+        //     top); the busiest queue's newest <= 32 run next (reference
+        //     push_batch keeps the newest 32 of k_max); the oldest entries are
+        //     written to the deque when a stack overflows or some worker is
+        //     hungry (always, with eager publication).  Slot stores only: the
+        //     fence in (3) publishes them.
+        int kn = -1;
         {
             const int Q = A.num_queues;
             // eager publication behaves as if some worker were always hungry
             const int hungry = A.publish_lazy ? __shfl_sync(0xffffffffu, hv, 0) : 1;
             const int reserve = A.publish_lazy ? kReserve : 0;
-            int kmax = -1, best = 0;
+            int best = 0;
             for (int k = 0; k < Q; ++k)
                 if (S.cnt[k] > best) {
                     best = S.cnt[k];
-                    kmax = k;
+                    kn = k;
                 }
             for (int k = 0; k < Q; ++k) {
                 const int n = min(S.cnt[k], A.spawn_cap);
@@ -936,9 +959,9 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
                 int from_sb = 0;
                 if (over > 0) {
                     const int m1 = min(over, size);
-                    if (m1 > 0) publish_src(A, S, k, ls, lo, kLocalCap - 1, m1);
+                    if (m1 > 0) publish_stage(A, S, k, ls, lo, kLocalCap - 1, m1);
                     from_sb = over - m1;
-                    if (from_sb > 0) publish_src(A, S, k, sb, 0, 0xFFFFFFFFu, from_sb);
+                    if (from_sb > 0) publish_stage(A, S, k, sb, 0, 0xFFFFFFFFu, from_sb);
                     if (lane == 0) S.ls_lo[k] = lo + (unsigned)m1;
                 }
                 for (int e = from_sb + (int)lane; e < n; e += 32)
@@ -947,7 +970,6 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
                 if (lane == 0) S.ls_hi[k] = hi + (unsigned)(n - from_sb);
                 __syncwarp();
             }
-            int kn = kmax;
             if (kn < 0) {
                 for (int kk = 0; kk < Q; ++kk) {
                     const int k = (S.cur_q + kk) % Q;
@@ -984,12 +1006,124 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
                     const int size = (int)(hi - lo);
                     const int m = size - reserve;
                     if (m > 0) {
-                        publish_src(A, S, k, S.lstk + k * kLocalCap, lo, kLocalCap - 1, m);
+                        publish_stage(A, S, k, S.lstk + k * kLocalCap, lo, kLocalCap - 1, m);
                         if (lane == 0) S.ls_lo[k] = lo + (unsigned)m;
                         __syncwarp();
                     }
                 }
             }
+        }
+        GTAP_PHASE_MARK(ph3);
+        GTAP_PHASE_ADD(12, ph2, ph3);
+        // (3) one warp-wide fence orders this round's stores (children's
+        //     records, results written into parents' frames, orphan marks,
+        //     deque slots) before the publication and before the join
+        //     decrements, which therefore need only acquire semantics.
+        const unsigned joiners = __ballot_sync(0xffffffffu, my_fin && S.l_parent[lane] >= 0);
+        publish_commit(A, S, joiners != 0);
+        GTAP_PHASE_MARK(ph3b);
+        GTAP_PHASE_ADD(7, ph3, ph3b);
+        // (4) joins: the last child re-enqueues its parent on the resume queue;
+        //     release the finished task's id unless its parent reads its frame
+        int resumed = -1, rq = 0;
+        if (my_fin) {
+            const int parent = S.l_parent[lane];
+            if (parent >= 0) {
+                const int old = atom_add_acquire(&hdr_of(A, parent)->join, -1);
+                if ((old & kJoinCountMask) == 1) {
+                    rq = (old >> 24) & 7;
+                    if (rq >= A.num_queues) rq = 0;
+                    resumed = parent;
+                }
+            }
+            if (!(lane_flags & kLaneRetain)) {
+                rt_release_id_dbg(A, my_tid);
+                rt_release_id(S, my_tid);
+            }
+        }
+        // (5) resumed parents take the free lanes of the next batch when they
+        //     belong to its queue; the others go on top of their queue's stack
+        const unsigned rmask = __ballot_sync(0xffffffffu, resumed >= 0);
+        if (rmask) {
+            if (nb_next == 0) kn = __shfl_sync(0xffffffffu, rq, __ffs(rmask) - 1);
+            const unsigned inb = __ballot_sync(0xffffffffu, resumed >= 0 && rq == kn);
+            const int room = 32 - nb_next;
+            const int nin = min(__popc(inb), room);
+            if ((int)lane >= nb_next && (int)lane < nb_next + nin) {
+                const int src = (int)__fns(inb, 0, (int)lane - nb_next + 1);
+                next_tid = -2 - src;   // filled from lane src below
+            }
+            const int v = __shfl_sync(0xffffffffu, resumed, next_tid <= -2 ? -2 - next_tid : 0);
+            if (next_tid <= -2) next_tid = v;
+            // resumed lanes that did not get a slot: all but the first nin of inb
+            const unsigned placed = nin > 0 ? (inb & ((2u << __fns(inb, 0, nin)) - 1u)) : 0u;
+            const unsigned rest = rmask & ~placed;
+            if (nin > 0 && lane == 0) S.cur_q = kn;
+            nb_next += nin;
+            for (int k = 0; rest && k < A.num_queues; ++k) {
+                const unsigned mk = __ballot_sync(0xffffffffu, ((rest >> lane) & 1u) && rq == k);
+                if (!mk) continue;
+                int* ls = S.lstk + k * kLocalCap;
+                const unsigned lo = S.ls_lo[k], hi = S.ls_hi[k];
+                const int add = __popc(mk);
+                const int over = (int)(hi - lo) + add - kLocalCap;
+                if (over > 0) {   // a full stack: its oldest entries go to the deque first (rare)
+                    publish_stage(A, S, k, ls, lo, kLocalCap - 1, over);
+                    publish_commit(A, S, false);
+                    if (lane == 0) S.ls_lo[k] = lo + (unsigned)over;
+                }
+                if ((mk >> lane) & 1u) ls[(hi + (unsigned)__popc(mk & ((1u << lane) - 1u))) & (kLocalCap - 1)] = resumed;
+                __syncwarp();
+                if (lane == 0) S.ls_hi[k] = hi + (unsigned)add;
+                __syncwarp();
+            }
+        }
+        GTAP_PHASE_MARK(ph4);
+        GTAP_PHASE_ADD(13, ph3b, ph4);
+        // (6) per-root accounting, one leader per distinct root
+        const int r0 = S.l_root[0];   // lane 0 always runs a task when nb > 0
+        if (__all_sync(0xffffffffu, !active || S.l_root[lane] == r0)) {
+            // every task of the round belongs to one root: warp sums, lane 0 books them
+            const unsigned created = active ? (unsigned)S.l_created[lane] : 0u;
+            const unsigned value = active ? (unsigned)S.l_value[lane] : 0u;
+            const int c_sum = (int)__reduce_add_sync(0xffffffffu, created);
+            const int f_sum = __popc(fin);
+            const int v_sum = (int)__reduce_add_sync(0xffffffffu, value);
+            if (lane == 0) {
+                if (v_sum) atomicAdd(reinterpret_cast<unsigned long long*>(&A.results[r0].value),
+                                     (unsigned long long)(long long)v_sum);
+                account_root(A, S, r0, c_sum, f_sum);
+                if (S.nbal > 1) age_bal(A, S);
+                else S.bal[0].touched = 0;
+            }
+            __syncwarp();
+        } else {
+            const int created = active ? S.l_created[lane] : 0;
+            const int finished = my_fin ? 1 : 0;
+            const int value = active ? S.l_value[lane] : 0;
+            const int r = active ? S.l_root[lane] : -1;
+            unsigned grp = __match_any_sync(0xffffffffu, r);
+            int c_sum = created, f_sum = finished, v_sum = value;
+            if (active) {
+                c_sum = (int)__reduce_add_sync(grp, (unsigned)created);
+                f_sum = (int)__reduce_add_sync(grp, (unsigned)finished);
+                v_sum = (int)__reduce_add_sync(grp, (unsigned)value);
+            }
+            const bool leader = active && ((unsigned)__ffs(grp) - 1u == lane);
+            unsigned leaders = __ballot_sync(0xffffffffu, leader);
+            __syncwarp();
+            while (leaders) {
+                const unsigned l = (unsigned)__ffs(leaders) - 1u;
+                if (lane == l) {
+                    if (v_sum) atomicAdd(reinterpret_cast<unsigned long long*>(&A.results[r].value),
+                                         (unsigned long long)(long long)v_sum);
+                    account_root(A, S, r, c_sum, f_sum);
+                }
+                __syncwarp();
+                leaders &= leaders - 1u;
+            }
+            if (lane == 0) age_bal(A, S);
+            __syncwarp();
         }
         __syncwarp();
         if (lane == 0) {
@@ -999,8 +1133,12 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
         }
         const unsigned created_all = __reduce_add_sync(0xffffffffu, (unsigned)(active ? S.l_created[lane] : 0));
         if (lane == 0) S.st[GTAP_STAT_TASKS] += created_all;
+        GTAP_PHASE_MARK(ph5);
+        GTAP_PHASE_ADD(14, ph4, ph5);
         // (6) id cache
         id_cache_maintain(A, S);
+        GTAP_PHASE_MARK(ph6);
+        GTAP_PHASE_ADD(15, ph5, ph6);
         nb = nb_next;
         my_tid = next_tid;
         next_tid = -1;
@@ -1038,6 +1176,7 @@ __device__ __forceinline__ void thread_worker_run(const Arena& A, WarpShared& S,
             S.ls_hi[k] = 0;
             S.cnt[k] = 0;
             S.bottom[k] = 0;
+            S.pend[k] = 0;
             S.top_cache[k] = 0;
         }
         S.cur_q = 0;
@@ -1047,10 +1186,6 @@ __device__ __forceinline__ void thread_worker_run(const Arena& A, WarpShared& S,
         S.nbal = 0;
         S.prof_h = 0;
         S.prof_w = 0;
-        S.fin_mask = 0;
-        S.retain_mask = 0;
-        S.leaf_mask = 0;
-        S.spawn_mask = 0;
         for (int i = 0; i < GTAP_STAT_COUNT; ++i) S.st[i] = 0;
     }
     // first ids come from the private range
