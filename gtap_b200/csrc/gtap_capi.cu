@@ -124,8 +124,15 @@ int ilog2_ceil(long long v) {
     return l;
 }
 
-const void* kernel_full() { return reinterpret_cast<const void*>(&thread_worker_kernel<BuiltinProgram>); }
-const void* kernel_light() { return reinterpret_cast<const void*>(&thread_worker_kernel_lb<BuiltinProgramLight>); }
+// Each variant exists for one queue (fewest registers) and for up to kMaxQueues.
+const void* kernel_full(int num_queues) {
+    return num_queues == 1 ? reinterpret_cast<const void*>(&thread_worker_kernel<BuiltinProgram, 1>)
+                           : reinterpret_cast<const void*>(&thread_worker_kernel<BuiltinProgram, kMaxQueues>);
+}
+const void* kernel_light(int num_queues) {
+    return num_queues == 1 ? reinterpret_cast<const void*>(&thread_worker_kernel_lb<BuiltinProgramLight, 1>)
+                           : reinterpret_cast<const void*>(&thread_worker_kernel_lb<BuiltinProgramLight, kMaxQueues>);
+}
 
 // Roots are admitted while at least this many task ids are free (never used
 // or recycled).  Ids parked in private ranges and per-warp caches are not
@@ -145,8 +152,11 @@ bool roots_need_sorts(const gtap_root* roots, int n) {
 // launch the worker kernel variant; A.num_workers must match it
 cudaError_t launch_worker(const Arena& A, bool light, cudaStream_t s) {
     const int blocks = A.num_workers / g.warps_per_block;
-    if (light) thread_worker_kernel_lb<BuiltinProgramLight><<<blocks, g.cfg.block, g.smem_bytes, s>>>(A);
-    else thread_worker_kernel<BuiltinProgram><<<blocks, g.cfg.block, g.smem_bytes, s>>>(A);
+    const bool one = g.cfg.num_queues == 1;
+    if (light && one) thread_worker_kernel_lb<BuiltinProgramLight, 1><<<blocks, g.cfg.block, g.smem_bytes, s>>>(A);
+    else if (light) thread_worker_kernel_lb<BuiltinProgramLight, kMaxQueues><<<blocks, g.cfg.block, g.smem_bytes, s>>>(A);
+    else if (one) thread_worker_kernel<BuiltinProgram, 1><<<blocks, g.cfg.block, g.smem_bytes, s>>>(A);
+    else thread_worker_kernel<BuiltinProgram, kMaxQueues><<<blocks, g.cfg.block, g.smem_bytes, s>>>(A);
     return cudaGetLastError();
 }
 
@@ -459,10 +469,10 @@ static int initialize_impl(const gtap_config* cfg_in, int external_workers) {
     GT_CUDA(cudaDeviceGetAttribute(&g.sm_count, cudaDevAttrMultiProcessorCount, g.device));
     const size_t smem = smem_for(c);
     int per_sm_full = 0, per_sm_light = 0;
-    GT_CUDA(cudaFuncSetAttribute(kernel_full(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    GT_CUDA(cudaFuncSetAttribute(kernel_light(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    GT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_full, kernel_full(), c.block, smem));
-    GT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_light, kernel_light(), c.block, smem));
+    GT_CUDA(cudaFuncSetAttribute(kernel_full(c.num_queues), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    GT_CUDA(cudaFuncSetAttribute(kernel_light(c.num_queues), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    GT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_full, kernel_full(c.num_queues), c.block, smem));
+    GT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_light, kernel_light(c.num_queues), c.block, smem));
     if (per_sm_light < 1) return GTAP_ERROR_INVALID_ARGUMENT;
     // one resident wave per variant; grid = 0 fills the GPU, otherwise cap it
     auto pick = [&](int per_sm) {

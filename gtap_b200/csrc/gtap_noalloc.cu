@@ -122,7 +122,7 @@ int setup_device(int dev, DeviceSetup& d) {
     void* ptr = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
     if (e != cudaSuccess) return -(int)e;
-    const void* kfn = reinterpret_cast<const void*>(&thread_worker_kernel_lb<BuiltinProgramLight>);
+    const void* kfn = reinterpret_cast<const void*>(&thread_worker_kernel_lb<BuiltinProgramLight, 1>);
     const size_t smem = noalloc_smem();
     e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return -(int)e;
@@ -232,7 +232,7 @@ extern "C" int gtap_launch_noalloc(const gtap_root* d_roots, int32_t n_roots, gt
     noalloc_reset_kernel<<<64, 256, 0, s>>>(A, counters, n_roots, W * kNoallocIdsPerWorker);
     e = cudaGetLastError();
     if (e != cudaSuccess) return -(int)e;
-    thread_worker_kernel_lb<BuiltinProgramLight><<<W / A.warps_per_block, kNoallocBlock, d.smem, s>>>(A);
+    thread_worker_kernel_lb<BuiltinProgramLight, 1><<<W / A.warps_per_block, kNoallocBlock, d.smem, s>>>(A);
     e = cudaGetLastError();
     if (e != cudaSuccess) return -(int)e;
     int status = 0;

@@ -23,7 +23,7 @@ struct SelftestCounters {
 
 // mode bits select the consumers active while tokens are produced:
 // 1 = own-deque pops, 2 = steals, 4 = overflow-queue reads (all run in the drain)
-static __global__ void selftest_queue_kernel(const Arena A, int rounds, int per_round_max, unsigned* seen,
+static __global__ void selftest_queue_kernel(const __grid_constant__ Arena A, int rounds, int per_round_max, unsigned* seen,
                                       SelftestCounters* c, int mode) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int wib = threadIdx.x >> 5;
@@ -36,14 +36,13 @@ static __global__ void selftest_queue_kernel(const Arena A, int rounds, int per_
         S.worker = worker;
         S.sbuf = sb_base + (size_t)wib * A.num_queues * A.spawn_cap;
         for (int k = 0; k < kMaxQueues; ++k) {
-            S.bottom[k] = 0;
-            S.pend[k] = 0;
-            S.top_cache[k] = 0;
             S.cnt[k] = 0;
         }
         for (int i = 0; i < GTAP_STAT_COUNT; ++i) S.st[i] = 0;
     }
     __syncwarp();
+    QueuePos<kMaxQueues> P;
+    queue_pos_init(P);
     unsigned rng = 0x2545F491u ^ (unsigned)(worker * 2654435761u) ^ (lane * 0x9E3779B9u);
     if (rng == 0) rng = 1;
     int last_victim = -1;
@@ -65,11 +64,11 @@ static __global__ void selftest_queue_kernel(const Arena A, int rounds, int per_
         for (int e = (int)lane; e < m; e += 32) S.sbuf[e] = (int)((unsigned)worker * 16384u + seq + (unsigned)e);
         __syncwarp();
         seq += (unsigned)m;
-        if (m > 0) publish_src(A, S, 0, S.sbuf, 0, 0xFFFFFFFFu, m);
+        if (m > 0) publish_src(A, S, P, 0, S.sbuf, 0, 0xFFFFFFFFu, m);
         int tok = -1;
         int got = 0;
         if (mode & 1) {
-            got = pop_own(A, S, 0, tok);
+            got = pop_own(A, S, P, 0, tok);
             consume(got, tok);
         }
         if ((mode & 2) && ((draw >> 8) & 1u)) {
@@ -89,7 +88,7 @@ static __global__ void selftest_queue_kernel(const Arena A, int rounds, int per_
     // drain: pop, steal and read the ring until every token is accounted for
     for (int spin = 0; spin < (1 << 20); ++spin) {
         int tok = -1;
-        int g1 = pop_own(A, S, 0, tok);
+        int g1 = pop_own(A, S, P, 0, tok);
         consume(g1, tok);
         int g2 = steal(A, S, 0, rng, last_victim, tok);
         consume(g2, tok);

@@ -55,8 +55,10 @@ namespace gtap {
 #define GTAP_PHASE_ADD(slot, t0, t1) (void)0
 #endif
 
-constexpr int kAvailCap = 256;    // per-warp cache of free task ids
-constexpr int kAvailHigh = 240;   // above this, 32 ids go back to the recycled pool
+constexpr int kAvailCap = 256;    // per-warp stack of free task ids
+constexpr int kAvailHigh = 224;   // above this, the oldest 32 go back to the recycled pool
+constexpr int kAvailLow = 64;     // below this, the stack is refilled ...
+constexpr int kAvailRefill = 96;  // ... by up to this many ids
 constexpr int kFreedCap = 96;
 constexpr int kRootBalCap = 8;
 constexpr int kBalChunk = 1024;
@@ -89,12 +91,9 @@ struct WarpShared {
     int l_value[kWarp];        // contributions to the lane's root value (n-queens counts)
     int l_flags[kWarp];        // this round, per lane: kLaneFinished | kLaneRetain | kLaneLeaf
     int cnt[kMaxQueues];       // children staged this round, per queue
-    unsigned bottom[kMaxQueues];
-    int pend[kMaxQueues];      // deque entries written this round, not yet published (publish_commit)
-    unsigned top_cache[kMaxQueues];
-    int cur_q;                 // EPAQ queue to try first (reference ctx->queue_idx)
-    int avail_n, alloc_pos, freed_n, bump;
-    int alloc_last;            // ids this warp allocated last round (refill target)
+    int avail_n;               // free ids on the stack avail[0, avail_n); below 0 within a round = overdrawn
+    int freed_n;               // ids released this round (freed[0, freed_n))
+    int bump;                  // next unused id of this warp's private range
     int avail[kAvailCap];
     int freed[kFreedCap];
     int nbal;
@@ -104,9 +103,56 @@ struct WarpShared {
     int prof_h, prof_w;
     int* sbuf;                 // [num_queues][spawn_cap] staged child ids (| spawner lane << 27)
     int* lstk;                 // [num_queues][kLocalCap] ready tasks not yet visible to thieves
-    unsigned ls_lo[kMaxQueues];   // oldest entry (published first)
-    unsigned ls_hi[kMaxQueues];   // one past the newest entry (run first)
 };
+
+// Positions of this warp's local stacks and deques.  Only the scheduler
+// changes them, identically in every lane: each lane keeps its own copy, so
+// no lane waits for another to publish an update through shared memory.
+// QM: the most queues the kernel supports (1 or kMaxQueues); fewer entries
+// fewer registers.
+template <int QM>
+struct QueuePos {
+    unsigned ls_lo[QM];      // local stack: oldest entry (published first)
+    unsigned ls_hi[QM];      // local stack: one past the newest entry (run first)
+    unsigned bottom[QM];     // deque bottom, entries staged this round included
+    unsigned top_cache[QM];  // deque top last read (it only grows)
+    int pend[QM];            // deque entries staged this round, not yet published
+    int cur_q;               // EPAQ queue to try first (reference ctx->queue_idx)
+};
+
+// Element k of a per-queue array through constant indices only, so that
+// QueuePos stays in registers instead of local memory.
+template <class T, int N>
+__device__ __forceinline__ T qget(const T (&a)[N], int k) {
+    T v = a[0];
+#pragma unroll
+    for (int i = 1; i < N; ++i)
+        if (k == i) v = a[i];
+    return v;
+}
+template <class T>
+struct QNoDeduce {
+    using type = T;
+};
+template <class T, int N>
+__device__ __forceinline__ void qset(T (&a)[N], int k, typename QNoDeduce<T>::type v) {
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+        if (k == i) a[i] = v;
+}
+
+template <int QM>
+__device__ __forceinline__ void queue_pos_init(QueuePos<QM>& P) {
+#pragma unroll
+    for (int k = 0; k < QM; ++k) {
+        qset(P.ls_lo, k, 0);
+        qset(P.ls_hi, k, 0);
+        qset(P.bottom, k, 0);
+        qset(P.top_cache, k, 0);
+        qset(P.pend, k, 0);
+    }
+    P.cur_q = 0;
+}
 
 struct TaskCtxT {
     const Arena* A;
@@ -155,92 +201,102 @@ __device__ __forceinline__ int warp_agg_inc(int* p, unsigned m) {
     return base + __popc(m & ((1u << lane) - 1u));
 }
 
+// Pop from the top of the free-id stack (the most recently freed ids: their
+// records are the warmest in L1/L2); the lanes of one call share one atomic.
 __device__ __forceinline__ int alloc_id(const Arena& A, WarpShared& S) {
-    const int a = warp_agg_inc(&S.alloc_pos, __activemask());
-    if (a < S.avail_n) return S.avail[a];
+    const unsigned m = __activemask();
+    const unsigned lane = lane_id();
+    const int leader = __ffs(m) - 1;
+    int top = 0;
+    if ((int)lane == leader) top = atomicSub(&S.avail_n, __popc(m));
+    top = __shfl_sync(m, top, leader);
+    const int i = top - 1 - __popc(m & ((1u << lane) - 1u));
+    if (i >= 0) return S.avail[i];
     return alloc_id_slow(A, S);
 }
 
-// Warp-cooperative: compact the cache after a round, return surplus ids to
-// the global ring and refill from the private range / ring / fresh ids.
+// Warp-cooperative, after a round: this round's freed ids go on top of the
+// stack (reused first); the stack is kept between kAvailLow and the
+// surplus mark by taking ids from the private range, the recycled-id ring or
+// fresh ids (placed underneath) and by returning the oldest ids to the ring.
 static __device__ void id_cache_maintain(const Arena& A, WarpShared& S) {
     const unsigned lane = lane_id();
     __syncwarp();
-    int consumed = min(S.alloc_pos, S.avail_n);
-    int remain = S.avail_n - consumed;
-    int nfreed = min(S.freed_n, kFreedCap);
-    const int used_this_round = S.alloc_pos;
-    // move remaining entries to the front (read all, then write)
-    int v[kAvailCap / 32];
-#pragma unroll
-    for (int j = 0; j < kAvailCap / 32; ++j)
-        v[j] = ((int)lane + 32 * j < remain) ? S.avail[consumed + lane + 32 * j] : 0;
-    __syncwarp();
-#pragma unroll
-    for (int j = 0; j < kAvailCap / 32; ++j)
-        if ((int)lane + 32 * j < remain) S.avail[lane + 32 * j] = v[j];
-    __syncwarp();
-    // append freed ids; whatever does not fit goes to the global ring
-    int n = remain;
+    int n = max(S.avail_n, 0);
+    const int nfreed = min(S.freed_n, kFreedCap);
+    // freed ids on top; whatever does not fit goes to the recycled-id ring
     for (int base = 0; base < nfreed; base += 32) {
-        int i = base + (int)lane;
-        int id = (i < nfreed) ? S.freed[i] : -1;
-        int take = min(32, nfreed - base);
-        int room = kAvailCap - n;
-        if (take <= room) {
+        const int take = min(32, nfreed - base);
+        const int id = ((int)lane < take) ? S.freed[base + lane] : -1;
+        if (take <= kAvailCap - n) {
             if ((int)lane < take) S.avail[n + lane] = id;
             n += take;
         } else {
-            // push this chunk of freed ids to the recycled-id ring
             ring_push_warp(A, A.idpool, id, take);
         }
-        __syncwarp();
     }
-    // surplus: give 32 back
+    __syncwarp();
+    // surplus: the oldest 32 go back to the ring, the rest slide down
     if (n > min(kAvailHigh, A.avail_target + 32)) {
-        int id = S.avail[n - 32 + lane];
+        ring_push_warp(A, A.idpool, S.avail[lane], 32);
+        int v[kAvailCap / 32];
+#pragma unroll
+        for (int j = 0; j < kAvailCap / 32; ++j) v[j] = (32 + (int)lane + 32 * j < n) ? S.avail[32 + lane + 32 * j] : 0;
         __syncwarp();
-        ring_push_warp(A, A.idpool, id, 32);
+#pragma unroll
+        for (int j = 0; j < kAvailCap / 32; ++j)
+            if (32 + (int)lane + 32 * j < n) S.avail[lane + 32 * j] = v[j];
         n -= 32;
-    }
-    // refill to about twice the last round's demand
-    const int target = min(A.avail_target, max(64, 2 * used_this_round));
-    for (int chunk = 0; chunk < 6 && n < target; ++chunk) {
-        int got = 0;
-        // private range first (no memory traffic)
-        int b = S.bump;
-        if (b < A.ids_per_worker) {
-            int k = min(32, A.ids_per_worker - b);
-            if ((int)lane < k) S.avail[n + lane] = A.id_base + S.worker * A.ids_per_worker + b + lane;
-            got = k;
-            __syncwarp();
-            if (lane == 0) S.bump = b + k;
-        }
-        if (got == 0) {
-            int id = -1;
-            got = ring_pop_warp(A, A.idpool, 32, &id);
-            if ((int)lane < got) S.avail[n + lane] = id;
-        }
-        if (got == 0) {
-            unsigned f = 0;
-            if (lane == 0) f = atom_add_relaxed(A.fresh_next, 32u);
-            f = __shfl_sync(0xffffffffu, f, 0);
-            if (f < (unsigned)A.total_ids) {
-                int k = min(32, A.total_ids - (int)f);
-                if ((int)lane < k) S.avail[n + lane] = (int)f + lane;
-                got = k;
-            }
-        }
-        n += got;
-        if (got == 0) break;
         __syncwarp();
+    }
+    // refill below kAvailLow: new ids go underneath, so the warm ones stay on top
+    if (n < kAvailLow) {
+        const int want = min(A.avail_target, kAvailRefill) - n;
+        int got = 0;
+        for (int chunk = 0; chunk < kAvailRefill / 32 && got < want; ++chunk) {
+            int k = 0, id = -1;
+            // private range first (no memory traffic)
+            const int b = S.bump;
+            if (b < A.ids_per_worker) {
+                k = min(32, A.ids_per_worker - b);
+                id = A.id_base + S.worker * A.ids_per_worker + b + (int)lane;
+                __syncwarp();
+                if (lane == 0) S.bump = b + k;
+            }
+            if (k == 0) k = ring_pop_warp(A, A.idpool, 32, &id);
+            if (k == 0) {
+                unsigned f = 0;
+                if (lane == 0) f = atom_add_relaxed(A.fresh_next, 32u);
+                f = __shfl_sync(0xffffffffu, f, 0);
+                if (f < (unsigned)A.total_ids) {
+                    k = min(32, A.total_ids - (int)f);
+                    id = (int)f + (int)lane;
+                }
+            }
+            if (k == 0) break;
+            // compact this chunk's k ids behind the ones already gathered
+            const int pos = got + (int)lane;
+            if ((int)lane < k) S.freed[pos] = id;   // freed[] is free scratch here
+            got += k;
+            __syncwarp();
+        }
+        if (got > 0) {
+            // slide the stack up by `got` and put the new ids underneath
+            int v[kAvailCap / 32];
+#pragma unroll
+            for (int j = 0; j < kAvailCap / 32; ++j) v[j] = ((int)lane + 32 * j < n) ? S.avail[lane + 32 * j] : 0;
+            __syncwarp();
+#pragma unroll
+            for (int j = 0; j < kAvailCap / 32; ++j)
+                if ((int)lane + 32 * j < n) S.avail[got + lane + 32 * j] = v[j];
+            for (int e = (int)lane; e < got; e += 32) S.avail[e] = S.freed[e];
+            n += got;
+        }
     }
     __syncwarp();
     if (lane == 0) {
         S.avail_n = n;
-        S.alloc_pos = 0;
         S.freed_n = 0;
-        S.alloc_last = used_this_round;
     }
     __syncwarp();
 }
@@ -336,10 +392,18 @@ __device__ __forceinline__ void rt_release_id_dbg(const Arena& A, int tid) {
 #endif
 }
 
-__device__ __forceinline__ void rt_release_id(WarpShared& S, int tid) {
+// The id returns to this warp's free-id stack at round end; beyond kFreedCap
+// releases in one round it goes to the recycled-id ring at once, after a fence
+// that completes this lane's earlier accesses to the id's record (the next
+// owner rewrites it).
+__device__ __forceinline__ void rt_release_id(const Arena& A, WarpShared& S, int tid) {
     const int f = warp_agg_inc(&S.freed_n, __activemask());
-    if (f < kFreedCap) S.freed[f] = tid;
-    // an overfull freed list loses the id until the next launch resets the arena
+    if (f < kFreedCap) {
+        S.freed[f] = tid;
+    } else {
+        fence_acq_rel();
+        ring_push_one(A.idpool, tid);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -430,17 +494,18 @@ static __device__ void age_bal(const Arena& A, WarpShared& S) {
 // deque operations
 // ---------------------------------------------------------------------------
 // Owner pop: LIFO, up to 32 newest published tasks of queue k.
-static __device__ int pop_own(const Arena& A, WarpShared& S, int k, int& my_tid) {
+template <int QM>
+static __device__ int pop_own(const Arena& A, WarpShared& S, QueuePos<QM>& P, int k, int& my_tid) {
     const unsigned lane = lane_id();
-    if (((S.bottom[k] - S.top_cache[k]) & kPosMask) == 0) return 0;  // top only grows: surely empty
+    if (((qget(P.bottom, k) - qget(P.top_cache, k)) & kPosMask) == 0) return 0;  // top only grows: surely empty
     int got = 0;
-    unsigned b = 0;
+    unsigned b = 0, top = qget(P.top_cache, k);
     if (lane == 0) {
         unsigned long long* c = dq_ctl_ptr(A, k, S.worker);
         unsigned long long wv = ld_relaxed(c);
         for (int i = 0; i < 16; ++i) {
             unsigned sz = dq_size(wv);
-            S.top_cache[k] = dq_top(wv);
+            top = dq_top(wv);
             if (sz == 0) break;
             unsigned take = sz < 32u ? sz : 32u;
             unsigned long long old = atom_cas_acquire(c, wv, dq_owner_pop(wv, take));
@@ -451,19 +516,18 @@ static __device__ int pop_own(const Arena& A, WarpShared& S, int k, int& my_tid)
                 if (take > sz || sz > (1u << A.deque_cap_log2)) GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, (int)take, k, 23, (int)sz);
 #endif
 #ifdef GTAP_DEBUG_IDS
-                if (b != S.bottom[k]) GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, (int)b, k, 11, (int)S.bottom[k]);
+                if (b != qget(P.bottom, k)) GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, (int)b, k, 11, (int)qget(P.bottom, k));
 #endif
                 break;
             }
             wv = old;
         }
-        if (got) {
-            S.bottom[k] = (b - (unsigned)got) & kPosMask;
-            S.st[GTAP_STAT_POPS] += 1;
-        }
+        if (got) S.st[GTAP_STAT_POPS] += 1;
     }
     got = __shfl_sync(0xffffffffu, got, 0);
     b = __shfl_sync(0xffffffffu, b, 0);
+    qset(P.top_cache, k, __shfl_sync(0xffffffffu, top, 0));
+    if (got) qset(P.bottom, k, (b - (unsigned)got) & kPosMask);
     if ((int)lane < got) {
         my_tid = ld_relaxed(dq_slot_ptr(A, k, S.worker, b - (unsigned)got + lane));
 #ifdef GTAP_DEBUG_IDS
@@ -570,19 +634,19 @@ static __device__ int steal(const Arena& A, WarpShared& S, int k, unsigned& rng,
 // Write m entries src[(start + i) & mask] into this warp's deque of queue k
 // (the owner's bottom moves at once; thieves see them only after
 // publish_commit), spilling to the overflow queue when the deque is full.
-static __device__ void publish_stage(const Arena& A, WarpShared& S, int k, const int* base, unsigned start,
-                                     unsigned mask, int m) {
+template <int QM>
+static __device__ void publish_stage(const Arena& A, WarpShared& S, QueuePos<QM>& P, int k, const int* base,
+                                     unsigned start, unsigned mask, int m) {
     const unsigned lane = lane_id();
     const unsigned cap = 1u << A.deque_cap_log2;
     auto src = [&](int i) { return base[(start + (unsigned)i) & mask]; };
-    unsigned used = (S.bottom[k] - S.top_cache[k]) & kPosMask;
+    unsigned used = (qget(P.bottom, k) - qget(P.top_cache, k)) & kPosMask;
     if (used + (unsigned)m > cap) {
         unsigned long long wv = 0;
         if (lane == 0) wv = ld_relaxed(dq_ctl_ptr(A, k, S.worker));
         wv = __shfl_sync(0xffffffffu, wv, 0);
-        if (lane == 0) S.top_cache[k] = dq_top(wv);
-        __syncwarp();
-        used = (S.bottom[k] - S.top_cache[k]) & kPosMask;
+        qset(P.top_cache, k, dq_top(wv));
+        used = (qget(P.bottom, k) - qget(P.top_cache, k)) & kPosMask;
     }
     int direct = m;
     if (used + (unsigned)m > cap) direct = (int)(cap - used);
@@ -590,14 +654,14 @@ static __device__ void publish_stage(const Arena& A, WarpShared& S, int k, const
     if (lane == 0 && used > cap) GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, (int)used, k, 20, (int)cap);
 #endif
     if (direct > 0) {
-        const unsigned b = S.bottom[k];
+        const unsigned b = qget(P.bottom, k);
 #ifdef GTAP_QUEUE_CHECKS
         if (lane == 0) {
             unsigned long long w = ld_relaxed(dq_ctl_ptr(A, k, S.worker));
-            if (((dq_bottom(w) + (unsigned)S.pend[k]) & kPosMask) != b)
+            if (((dq_bottom(w) + (unsigned)qget(P.pend, k)) & kPosMask) != b)
                 GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, (int)dq_bottom(w), k, 21, (int)b);
             if (((b - dq_top(w)) & kPosMask) + (unsigned)direct > cap)
-                GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, (int)dq_top(w), k, 24, (int)S.top_cache[k]);
+                GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, (int)dq_top(w), k, 24, (int)qget(P.top_cache, k));
         }
 #endif
         for (int e = (int)lane; e < direct; e += 32) {
@@ -608,11 +672,8 @@ static __device__ void publish_stage(const Arena& A, WarpShared& S, int k, const
             A.dbg_slotpos[dq_slot_ptr(A, k, S.worker, pos) - A.dq_slots] = pos;
 #endif
         }
-        __syncwarp();
-        if (lane == 0) {
-            S.bottom[k] = (b + (unsigned)direct) & kPosMask;
-            S.pend[k] += direct;
-        }
+        qset(P.bottom, k, (b + (unsigned)direct) & kPosMask);
+        qset(P.pend, k, qget(P.pend, k) + (direct));
     }
     // the rest spills to the global overflow queue (its own fence: rare)
     for (int base_i = direct; base_i < m; base_i += 32) {
@@ -627,40 +688,45 @@ static __device__ void publish_stage(const Arena& A, WarpShared& S, int k, const
         if (lane == 0) S.st[GTAP_STAT_OVERFLOW_PUSHES] += (unsigned long long)take;
 #endif
     }
-    __syncwarp();
+    __syncwarp();   // the source entries are read before any lane overwrites them
 }
 
 // One warp-wide fence orders every store this warp made so far (task
 // records, results, deque slots) before what follows; then lane 0 moves the
 // bottoms of the deques publish_stage wrote, making those entries stealable.
 // fence: also when nothing is pending (the joins that follow rely on it).
-static __device__ void publish_commit(const Arena& A, WarpShared& S, bool fence) {
+template <int QM>
+static __device__ void publish_commit(const Arena& A, WarpShared& S, QueuePos<QM>& P, bool fence) {
     const unsigned lane = lane_id();
     bool any = false;
-    for (int k = 0; k < A.num_queues; ++k) any |= S.pend[k] != 0;
+#pragma unroll
+    for (int k = 0; k < QM; ++k) any |= P.pend[k] != 0;
     if (!any && !fence) return;
     fence_acq_rel();
-    __syncwarp();
-    if (any && lane == 0) {
-        for (int k = 0; k < A.num_queues; ++k) {
-            const int d = S.pend[k];
-            if (d) {
-                red_add_relaxed(dq_ctl_ptr(A, k, S.worker), (unsigned long long)d << kPosBits);
+    __syncwarp();   // every lane's fence is done before lane 0 publishes
+    if (any) {
+        if (lane == 0) {
+            for (int k = 0; k < A.num_queues; ++k) {
+                const int d = qget(P.pend, k);
+                if (d) {
+                    red_add_relaxed(dq_ctl_ptr(A, k, S.worker), (unsigned long long)d << kPosBits);
 #ifndef GTAP_PHASE_TIMERS
-                S.st[GTAP_STAT_PUBLISHED] += (unsigned long long)d;
+                    S.st[GTAP_STAT_PUBLISHED] += (unsigned long long)d;
 #endif
-                S.pend[k] = 0;
+                }
             }
         }
+#pragma unroll
+        for (int k = 0; k < QM; ++k) P.pend[k] = 0;
     }
-    __syncwarp();
 }
 
 // Stage and publish at once.
-static __device__ void publish_src(const Arena& A, WarpShared& S, int k, const int* base, unsigned start,
+template <int QM>
+static __device__ void publish_src(const Arena& A, WarpShared& S, QueuePos<QM>& P, int k, const int* base, unsigned start,
                                    unsigned mask, int m) {
-    publish_stage(A, S, k, base, start, mask, m);
-    publish_commit(A, S, false);
+    publish_stage(A, S, P, k, base, start, mask, m);
+    publish_commit(A, S, P, false);
 }
 
 // ---------------------------------------------------------------------------
@@ -765,9 +831,11 @@ static __device__ int admit(const Arena& A, WarpShared& S, int& my_tid) {
 // ---------------------------------------------------------------------------
 // the persistent worker loop
 // ---------------------------------------------------------------------------
-template <class Prog>
+template <class Prog, int QM>
 static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_tid) {
     const unsigned lane = lane_id();
+    QueuePos<QM> P;
+    queue_pos_init(P);
     int my_tid = (initial_tid >= 0 && lane == 0) ? initial_tid : -1;
     int nb = initial_tid >= 0 ? 1 : 0;
     unsigned rng = 0x9E3779B9u ^ (unsigned)(S.worker * 2654435761u) ^ (lane * 0x85EBCA6Bu) ^ (unsigned)clock64();
@@ -795,15 +863,15 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
             // (reference :896-926), then the overflow queue, then new roots.
             const int Q = A.num_queues;
             for (int kk = 0; kk < Q && nb == 0; ++kk) {
-                int k = (S.cur_q + kk) % Q;
-                nb = pop_own(A, S, k, my_tid);
+                int k = (P.cur_q + kk) % Q;
+                nb = pop_own(A, S, P, k, my_tid);
                 src_kind = 1;
                 if (nb == 0) {
                     nb = steal(A, S, k, rng, last_victim, my_tid);
                     src_kind = 2;
                 }
                 if (nb) {
-                    if (lane == 0) S.cur_q = k;
+                    P.cur_q = k;
                 }
             }
             if (nb == 0) {
@@ -953,27 +1021,26 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
                 if (n == 0) continue;
                 const int* sb = S.sbuf + k * A.spawn_cap;
                 int* ls = S.lstk + k * kLocalCap;
-                const unsigned lo = S.ls_lo[k], hi = S.ls_hi[k];
+                const unsigned lo = qget(P.ls_lo, k), hi = qget(P.ls_hi, k);
                 const int size = (int)(hi - lo);
                 const int over = size + n - kLocalCap;
                 int from_sb = 0;
                 if (over > 0) {
                     const int m1 = min(over, size);
-                    if (m1 > 0) publish_stage(A, S, k, ls, lo, kLocalCap - 1, m1);
+                    if (m1 > 0) publish_stage(A, S, P, k, ls, lo, kLocalCap - 1, m1);
                     from_sb = over - m1;
-                    if (from_sb > 0) publish_stage(A, S, k, sb, 0, 0xFFFFFFFFu, from_sb);
-                    if (lane == 0) S.ls_lo[k] = lo + (unsigned)m1;
+                    if (from_sb > 0) publish_stage(A, S, P, k, sb, 0, 0xFFFFFFFFu, from_sb);
+                    qset(P.ls_lo, k, lo + (unsigned)m1);
                 }
                 for (int e = from_sb + (int)lane; e < n; e += 32)
                     ls[(hi + (unsigned)(e - from_sb)) & (kLocalCap - 1)] = sb[e] & kIdMask;
-                __syncwarp();
-                if (lane == 0) S.ls_hi[k] = hi + (unsigned)(n - from_sb);
-                __syncwarp();
+                qset(P.ls_hi, k, hi + (unsigned)(n - from_sb));
             }
+            __syncwarp();   // local-stack entries written above are read below by other lanes
             if (kn < 0) {
                 for (int kk = 0; kk < Q; ++kk) {
-                    const int k = (S.cur_q + kk) % Q;
-                    if (S.ls_hi[k] != S.ls_lo[k]) {
+                    const int k = (P.cur_q + kk) % Q;
+                    if (qget(P.ls_hi, k) != qget(P.ls_lo, k)) {
                         kn = k;
                         break;
                     }
@@ -982,7 +1049,7 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
             nb_next = 0;
             if (kn >= 0) {
                 int* ls = S.lstk + kn * kLocalCap;
-                const unsigned lo = S.ls_lo[kn], hi = S.ls_hi[kn];
+                const unsigned lo = qget(P.ls_lo, kn), hi = qget(P.ls_hi, kn);
                 const int size = (int)(hi - lo);
                 const int take = min(32, size);
                 nb_next = take;
@@ -992,23 +1059,18 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
                     if (ld_cg(&A.dbg_live[next_tid]) != 1) GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, next_tid, kn, 15, take);
 #endif
                 }
-                __syncwarp();
-                if (lane == 0) {
-                    S.ls_hi[kn] = hi - (unsigned)take;
-                    S.cur_q = kn;
-                }
-                __syncwarp();
+                qset(P.ls_hi, kn, hi - (unsigned)take);
+                P.cur_q = kn;
             }
             if (hungry > 0) {
                 // keep one more batch in reserve so the next rounds stay full
                 for (int k = 0; k < Q; ++k) {
-                    const unsigned lo = S.ls_lo[k], hi = S.ls_hi[k];
+                    const unsigned lo = qget(P.ls_lo, k), hi = qget(P.ls_hi, k);
                     const int size = (int)(hi - lo);
                     const int m = size - reserve;
                     if (m > 0) {
-                        publish_stage(A, S, k, S.lstk + k * kLocalCap, lo, kLocalCap - 1, m);
-                        if (lane == 0) S.ls_lo[k] = lo + (unsigned)m;
-                        __syncwarp();
+                        publish_stage(A, S, P, k, S.lstk + k * kLocalCap, lo, kLocalCap - 1, m);
+                        qset(P.ls_lo, k, lo + (unsigned)m);
                     }
                 }
             }
@@ -1020,7 +1082,7 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
         //     deque slots) before the publication and before the join
         //     decrements, which therefore need only acquire semantics.
         const unsigned joiners = __ballot_sync(0xffffffffu, my_fin && S.l_parent[lane] >= 0);
-        publish_commit(A, S, joiners != 0);
+        publish_commit(A, S, P, joiners != 0);
         GTAP_PHASE_MARK(ph3b);
         GTAP_PHASE_ADD(7, ph3, ph3b);
         // (4) joins: the last child re-enqueues its parent on the resume queue;
@@ -1038,7 +1100,7 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
             }
             if (!(lane_flags & kLaneRetain)) {
                 rt_release_id_dbg(A, my_tid);
-                rt_release_id(S, my_tid);
+                rt_release_id(A, S, my_tid);
             }
         }
         // (5) resumed parents take the free lanes of the next batch when they
@@ -1058,23 +1120,23 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
             // resumed lanes that did not get a slot: all but the first nin of inb
             const unsigned placed = nin > 0 ? (inb & ((2u << __fns(inb, 0, nin)) - 1u)) : 0u;
             const unsigned rest = rmask & ~placed;
-            if (nin > 0 && lane == 0) S.cur_q = kn;
+            if (nin > 0) P.cur_q = kn;
+            __syncwarp();   // batch entries were read from the local stacks before they are reused
             nb_next += nin;
             for (int k = 0; rest && k < A.num_queues; ++k) {
                 const unsigned mk = __ballot_sync(0xffffffffu, ((rest >> lane) & 1u) && rq == k);
                 if (!mk) continue;
                 int* ls = S.lstk + k * kLocalCap;
-                const unsigned lo = S.ls_lo[k], hi = S.ls_hi[k];
+                const unsigned lo = qget(P.ls_lo, k), hi = qget(P.ls_hi, k);
                 const int add = __popc(mk);
                 const int over = (int)(hi - lo) + add - kLocalCap;
                 if (over > 0) {   // a full stack: its oldest entries go to the deque first (rare)
-                    publish_stage(A, S, k, ls, lo, kLocalCap - 1, over);
-                    publish_commit(A, S, false);
-                    if (lane == 0) S.ls_lo[k] = lo + (unsigned)over;
+                    publish_stage(A, S, P, k, ls, lo, kLocalCap - 1, over);
+                    publish_commit(A, S, P, false);
+                    qset(P.ls_lo, k, lo + (unsigned)over);
                 }
                 if ((mk >> lane) & 1u) ls[(hi + (unsigned)__popc(mk & ((1u << lane) - 1u))) & (kLocalCap - 1)] = resumed;
-                __syncwarp();
-                if (lane == 0) S.ls_hi[k] = hi + (unsigned)add;
+                qset(P.ls_hi, k, hi + (unsigned)add);
                 __syncwarp();
             }
         }
@@ -1163,7 +1225,7 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
 // buffer sbuf and local stack lstk given by the caller), run the loop, write
 // its statistics.  initial_tid >= 0 starts lane 0 on that task (a task
 // created before the loop, e.g. by the drop-in __gtap_push_initial_task).
-template <class Prog>
+template <class Prog, int QM>
 __device__ __forceinline__ void thread_worker_run(const Arena& A, WarpShared& S, int worker, int* sbuf, int* lstk,
                                                   int initial_tid) {
     const unsigned lane = lane_id();
@@ -1171,17 +1233,7 @@ __device__ __forceinline__ void thread_worker_run(const Arena& A, WarpShared& S,
         S.worker = worker;
         S.sbuf = sbuf;
         S.lstk = lstk;
-        for (int k = 0; k < kMaxQueues; ++k) {
-            S.ls_lo[k] = 0;
-            S.ls_hi[k] = 0;
-            S.cnt[k] = 0;
-            S.bottom[k] = 0;
-            S.pend[k] = 0;
-            S.top_cache[k] = 0;
-        }
-        S.cur_q = 0;
-        S.alloc_last = 0;
-        S.alloc_pos = 0;
+        for (int k = 0; k < kMaxQueues; ++k) S.cnt[k] = 0;
         S.freed_n = 0;
         S.nbal = 0;
         S.prof_h = 0;
@@ -1198,36 +1250,39 @@ __device__ __forceinline__ void thread_worker_run(const Arena& A, WarpShared& S,
         S.bump = first;
     }
     __syncwarp();
-    worker_loop<Prog>(A, S, initial_tid);
+    worker_loop<Prog, QM>(A, S, initial_tid);
     __syncwarp();
     if ((int)lane < GTAP_STAT_COUNT) A.stats[(size_t)worker * GTAP_STAT_COUNT + lane] = S.st[lane];
 }
 
 // Kernel body: warps_per_block WarpShared records + staging buffers in dynamic smem.
-template <class Prog>
+template <class Prog, int QM>
 __device__ __forceinline__ void thread_worker_body(const Arena& A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int wib = threadIdx.x >> 5;
     WarpShared* ws = reinterpret_cast<WarpShared*>(smem_raw);
     int* sb_base = reinterpret_cast<int*>(smem_raw + sizeof(WarpShared) * A.warps_per_block);
     int* ls_base = sb_base + (size_t)A.warps_per_block * A.num_queues * A.spawn_cap;
-    thread_worker_run<Prog>(A, ws[wib], blockIdx.x * A.warps_per_block + wib,
+    thread_worker_run<Prog, QM>(A, ws[wib], blockIdx.x * A.warps_per_block + wib,
                             sb_base + (size_t)wib * A.num_queues * A.spawn_cap,
                             ls_base + (size_t)wib * A.num_queues * kLocalCap, -1);
 }
 
 
-// Register-unbounded kernel (sorting kinds need the 64-key register network).
-template <class Prog>
-__global__ void thread_worker_kernel(const Arena A) {
-    thread_worker_body<Prog>(A);
+// The arena descriptor stays in the kernel's parameter (constant) space:
+// __grid_constant__ lets the scheduler take its address without the compiler
+// copying its 400-odd bytes into every thread's local memory, where each field
+// read would be a local load that mostly misses L1.
+template <class Prog, int QM>
+__global__ void thread_worker_kernel(const __grid_constant__ Arena A) {
+    thread_worker_body<Prog, QM>(A);
 }
 
 // At most 64 registers per thread: any block size up to 1024 fits, and the
 // light program reaches 32 resident warps per SM.
-template <class Prog>
-__global__ void __launch_bounds__(1024, 1) thread_worker_kernel_lb(const Arena A) {
-    thread_worker_body<Prog>(A);
+template <class Prog, int QM>
+__global__ void __launch_bounds__(1024, 1) thread_worker_kernel_lb(const __grid_constant__ Arena A) {
+    thread_worker_body<Prog, QM>(A);
 }
 
 }  // namespace gtap

@@ -274,12 +274,12 @@ extern "C" __device__ __forceinline__ void __gtap_execute_task_loop_device() {
         sbuf = base;
         lstk = base + (size_t)GTAP_NUM_QUEUES * kSpawnCap;
     }
-    gtap::thread_worker_run<Program>(A, warp_state(), worker, sbuf, lstk, first);
+    gtap::thread_worker_run<Program, GTAP_NUM_QUEUES>(A, warp_state(), worker, sbuf, lstk, first);
 }
 
 extern "C" __device__ __forceinline__ void __gtap_release_task_id(int tid) {
     gtap::rt_release_id_dbg(gtap_dropin::arena, tid);
-    gtap::rt_release_id(gtap_dropin::warp_state(), tid);
+    gtap::rt_release_id(gtap_dropin::arena, gtap_dropin::warp_state(), tid);
 }
 
 __device__ __forceinline__ void* __gtap_get_task_data(int tid) { return gtap::frame_of(gtap_dropin::arena, tid); }
