@@ -55,10 +55,8 @@ namespace gtap {
 #define GTAP_PHASE_ADD(slot, t0, t1) (void)0
 #endif
 
-constexpr int kAvailCap = 256;    // per-warp stack of free task ids
-constexpr int kAvailHigh = 224;   // above this, the oldest 32 go back to the recycled pool
-constexpr int kAvailLow = 64;     // below this, the stack is refilled ...
-constexpr int kAvailRefill = 96;  // ... by up to this many ids
+constexpr int kAvailCap = 256;    // per-warp cache of free task ids
+constexpr int kAvailHigh = 240;   // above this, 32 ids go back to the recycled pool
 constexpr int kFreedCap = 96;
 constexpr int kRootBalCap = 8;
 constexpr int kBalChunk = 1024;
@@ -91,9 +89,8 @@ struct WarpShared {
     int l_value[kWarp];        // contributions to the lane's root value (n-queens counts)
     int l_flags[kWarp];        // this round, per lane: kLaneFinished | kLaneRetain | kLaneLeaf
     int cnt[kMaxQueues];       // children staged this round, per queue
-    int avail_n;               // free ids on the stack avail[0, avail_n); below 0 within a round = overdrawn
-    int freed_n;               // ids released this round (freed[0, freed_n))
-    int bump;                  // next unused id of this warp's private range
+    int avail_n, alloc_pos, freed_n, bump;
+    int alloc_last;            // ids this warp allocated last round (refill target)
     int avail[kAvailCap];
     int freed[kFreedCap];
     int nbal;
@@ -201,102 +198,92 @@ __device__ __forceinline__ int warp_agg_inc(int* p, unsigned m) {
     return base + __popc(m & ((1u << lane) - 1u));
 }
 
-// Pop from the top of the free-id stack (the most recently freed ids: their
-// records are the warmest in L1/L2); the lanes of one call share one atomic.
 __device__ __forceinline__ int alloc_id(const Arena& A, WarpShared& S) {
-    const unsigned m = __activemask();
-    const unsigned lane = lane_id();
-    const int leader = __ffs(m) - 1;
-    int top = 0;
-    if ((int)lane == leader) top = atomicSub(&S.avail_n, __popc(m));
-    top = __shfl_sync(m, top, leader);
-    const int i = top - 1 - __popc(m & ((1u << lane) - 1u));
-    if (i >= 0) return S.avail[i];
+    const int a = warp_agg_inc(&S.alloc_pos, __activemask());
+    if (a < S.avail_n) return S.avail[a];
     return alloc_id_slow(A, S);
 }
 
-// Warp-cooperative, after a round: this round's freed ids go on top of the
-// stack (reused first); the stack is kept between kAvailLow and the
-// surplus mark by taking ids from the private range, the recycled-id ring or
-// fresh ids (placed underneath) and by returning the oldest ids to the ring.
+// Warp-cooperative: compact the cache after a round, return surplus ids to
+// the global ring and refill from the private range / ring / fresh ids.
 static __device__ void id_cache_maintain(const Arena& A, WarpShared& S) {
     const unsigned lane = lane_id();
     __syncwarp();
-    int n = max(S.avail_n, 0);
-    const int nfreed = min(S.freed_n, kFreedCap);
-    // freed ids on top; whatever does not fit goes to the recycled-id ring
+    int consumed = min(S.alloc_pos, S.avail_n);
+    int remain = S.avail_n - consumed;
+    int nfreed = min(S.freed_n, kFreedCap);
+    const int used_this_round = S.alloc_pos;
+    // move remaining entries to the front (read all, then write)
+    int v[kAvailCap / 32];
+#pragma unroll
+    for (int j = 0; j < kAvailCap / 32; ++j)
+        v[j] = ((int)lane + 32 * j < remain) ? S.avail[consumed + lane + 32 * j] : 0;
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < kAvailCap / 32; ++j)
+        if ((int)lane + 32 * j < remain) S.avail[lane + 32 * j] = v[j];
+    __syncwarp();
+    // append freed ids; whatever does not fit goes to the global ring
+    int n = remain;
     for (int base = 0; base < nfreed; base += 32) {
-        const int take = min(32, nfreed - base);
-        const int id = ((int)lane < take) ? S.freed[base + lane] : -1;
-        if (take <= kAvailCap - n) {
+        int i = base + (int)lane;
+        int id = (i < nfreed) ? S.freed[i] : -1;
+        int take = min(32, nfreed - base);
+        int room = kAvailCap - n;
+        if (take <= room) {
             if ((int)lane < take) S.avail[n + lane] = id;
             n += take;
         } else {
+            // push this chunk of freed ids to the recycled-id ring
             ring_push_warp(A, A.idpool, id, take);
         }
+        __syncwarp();
     }
-    __syncwarp();
-    // surplus: the oldest 32 go back to the ring, the rest slide down
+    // surplus: give 32 back
     if (n > min(kAvailHigh, A.avail_target + 32)) {
-        ring_push_warp(A, A.idpool, S.avail[lane], 32);
-        int v[kAvailCap / 32];
-#pragma unroll
-        for (int j = 0; j < kAvailCap / 32; ++j) v[j] = (32 + (int)lane + 32 * j < n) ? S.avail[32 + lane + 32 * j] : 0;
+        int id = S.avail[n - 32 + lane];
         __syncwarp();
-#pragma unroll
-        for (int j = 0; j < kAvailCap / 32; ++j)
-            if (32 + (int)lane + 32 * j < n) S.avail[lane + 32 * j] = v[j];
+        ring_push_warp(A, A.idpool, id, 32);
         n -= 32;
-        __syncwarp();
     }
-    // refill below kAvailLow: new ids go underneath, so the warm ones stay on top
-    if (n < kAvailLow) {
-        const int want = min(A.avail_target, kAvailRefill) - n;
+    // refill to about twice the last round's demand
+    const int target = min(A.avail_target, max(64, 2 * used_this_round));
+    for (int chunk = 0; chunk < 6 && n < target; ++chunk) {
         int got = 0;
-        for (int chunk = 0; chunk < kAvailRefill / 32 && got < want; ++chunk) {
-            int k = 0, id = -1;
-            // private range first (no memory traffic)
-            const int b = S.bump;
-            if (b < A.ids_per_worker) {
-                k = min(32, A.ids_per_worker - b);
-                id = A.id_base + S.worker * A.ids_per_worker + b + (int)lane;
-                __syncwarp();
-                if (lane == 0) S.bump = b + k;
-            }
-            if (k == 0) k = ring_pop_warp(A, A.idpool, 32, &id);
-            if (k == 0) {
-                unsigned f = 0;
-                if (lane == 0) f = atom_add_relaxed(A.fresh_next, 32u);
-                f = __shfl_sync(0xffffffffu, f, 0);
-                if (f < (unsigned)A.total_ids) {
-                    k = min(32, A.total_ids - (int)f);
-                    id = (int)f + (int)lane;
-                }
-            }
-            if (k == 0) break;
-            // compact this chunk's k ids behind the ones already gathered
-            const int pos = got + (int)lane;
-            if ((int)lane < k) S.freed[pos] = id;   // freed[] is free scratch here
-            got += k;
+        // private range first (no memory traffic)
+        int b = S.bump;
+        if (b < A.ids_per_worker) {
+            int k = min(32, A.ids_per_worker - b);
+            if ((int)lane < k) S.avail[n + lane] = A.id_base + S.worker * A.ids_per_worker + b + lane;
+            got = k;
             __syncwarp();
+            if (lane == 0) S.bump = b + k;
         }
-        if (got > 0) {
-            // slide the stack up by `got` and put the new ids underneath
-            int v[kAvailCap / 32];
-#pragma unroll
-            for (int j = 0; j < kAvailCap / 32; ++j) v[j] = ((int)lane + 32 * j < n) ? S.avail[lane + 32 * j] : 0;
-            __syncwarp();
-#pragma unroll
-            for (int j = 0; j < kAvailCap / 32; ++j)
-                if ((int)lane + 32 * j < n) S.avail[got + lane + 32 * j] = v[j];
-            for (int e = (int)lane; e < got; e += 32) S.avail[e] = S.freed[e];
-            n += got;
+        if (got == 0) {
+            int id = -1;
+            got = ring_pop_warp(A, A.idpool, 32, &id);
+            if ((int)lane < got) S.avail[n + lane] = id;
         }
+        if (got == 0) {
+            unsigned f = 0;
+            if (lane == 0) f = atom_add_relaxed(A.fresh_next, 32u);
+            f = __shfl_sync(0xffffffffu, f, 0);
+            if (f < (unsigned)A.total_ids) {
+                int k = min(32, A.total_ids - (int)f);
+                if ((int)lane < k) S.avail[n + lane] = (int)f + lane;
+                got = k;
+            }
+        }
+        n += got;
+        if (got == 0) break;
+        __syncwarp();
     }
     __syncwarp();
     if (lane == 0) {
         S.avail_n = n;
+        S.alloc_pos = 0;
         S.freed_n = 0;
+        S.alloc_last = used_this_round;
     }
     __syncwarp();
 }
@@ -1234,6 +1221,8 @@ __device__ __forceinline__ void thread_worker_run(const Arena& A, WarpShared& S,
         S.sbuf = sbuf;
         S.lstk = lstk;
         for (int k = 0; k < kMaxQueues; ++k) S.cnt[k] = 0;
+        S.alloc_last = 0;
+        S.alloc_pos = 0;
         S.freed_n = 0;
         S.nbal = 0;
         S.prof_h = 0;
