@@ -920,13 +920,14 @@ extern "C" int gtap_serve_poll(int32_t* indices, int32_t max, int32_t* n_out) {
 extern "C" int gtap_serve_results(const int32_t* indices, int32_t n, gtap_root_result* out) {
     if (!g.serving && !g.initialized) return GTAP_ERROR_NOT_INITIALIZED;
     if (!indices || !out || n < 0) return GTAP_ERROR_INVALID_ARGUMENT;
+    // while serving, beside the running kernel; after shutdown, on the default stream
+    cudaStream_t s = g.serving ? g.feed_stream : nullptr;
     for (int i = 0; i < n; ++i) {
         int slot = indices[i];
         if (slot < 0 || slot >= g.root_cap) return GTAP_ERROR_INVALID_ARGUMENT;
-        GT_CUDA(cudaMemcpyAsync(out + i, g.d_results + slot, sizeof(gtap_root_result), cudaMemcpyDeviceToHost,
-                                g.feed_stream));
+        GT_CUDA(cudaMemcpyAsync(out + i, g.d_results + slot, sizeof(gtap_root_result), cudaMemcpyDeviceToHost, s));
     }
-    GT_CUDA(cudaStreamSynchronize(g.feed_stream));
+    GT_CUDA(cudaStreamSynchronize(s));
     return 0;
 }
 
@@ -950,6 +951,10 @@ extern "C" int gtap_serve_shutdown(gtap_run_stats* stats) {
     cudaEventDestroy(g.serve_ev1);
     cudaStreamDestroy(g.serve_stream);
     cudaStreamDestroy(g.feed_stream);
+    g.serve_stream = nullptr;
+    g.feed_stream = nullptr;
+    g.serve_ev0 = nullptr;
+    g.serve_ev1 = nullptr;
     cudaFreeHost(g.h_done_ring);
     cudaFreeHost(g.h_pub_src);
     cudaFreeHost(g.h_shutdown_src);

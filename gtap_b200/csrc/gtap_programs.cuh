@@ -702,11 +702,22 @@ struct BuiltinProgramT {
     }
 
     // Argument ranges the built-in tasks rely on: fib's serial leaf handles
-    // n <= 64, n-queens packs n and the cutoff into 8 bits with n <= 32 columns.
+    // n <= 64, n-queens packs n and the cutoff into 8 bits with n <= 32
+    // columns; the array kinds need their arrays, a count that fits int32 and
+    // a start node inside it.  A root that fails is recorded as an error and
+    // touches none of its arrays.
     __device__ static bool root_args_ok(const gtap_root& rd) {
         switch (rd.kind) {
             case GTAP_KIND_FIB: return rd.i0 <= 64;
             case GTAP_KIND_NQ: return rd.i0 >= 0 && rd.i0 <= 32 && rd.i1 >= 0 && rd.i1 < 256;
+            case GTAP_KIND_CILKSORT:
+            case GTAP_KIND_MERGESORT:
+                return rd.n >= 0 && rd.n <= 0x7FFFFFFF && (rd.n == 0 || (rd.p0 && rd.p1 && rd.p2));
+            case GTAP_KIND_BFS:
+                return rd.p0 && rd.p1 && rd.p2 && rd.n > 0 && rd.n <= 0x7FFFFFFF && rd.i0 >= 0 && rd.i0 < rd.n;
+            case GTAP_KIND_TREESUM:
+                return rd.p0 && rd.p1 && rd.p2 && rd.p3 && rd.n > 0 && rd.n <= 0x7FFFFFFF && rd.i0 >= 0 &&
+                       rd.i0 < rd.n;
             default: return true;
         }
     }

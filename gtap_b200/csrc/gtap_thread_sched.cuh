@@ -88,6 +88,7 @@ struct WarpShared {
     int l_created[kWarp];      // tasks this lane created this round
     int l_value[kWarp];        // contributions to the lane's root value (n-queens counts)
     int l_flags[kWarp];        // this round, per lane: kLaneFinished | kLaneRetain | kLaneLeaf
+    int l_pend[kWarp];         // detached child past the staging buffer whose frame is still being written (-1: none)
     int cnt[kMaxQueues];       // children staged this round, per queue
     int avail_n, alloc_pos, freed_n, bump;
     int alloc_last;            // ids this warp allocated last round (refill target)
@@ -293,9 +294,22 @@ static __device__ void id_cache_maintain(const Arena& A, WarpShared& S) {
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ int rt_state(const WarpShared& S) { return (int)(S.l_w0[lane_id()] & 0xFFFFu); }
 
+// A detached child that did not fit the staging buffer, once its frame is
+// written: the fence orders its record, frame and function pointer before the
+// id appears in the overflow queue.
+__device__ __forceinline__ void push_overflow_child(const Arena& A, WarpShared& S, int id) {
+    fence_acq_rel();
+    ring_push_one(A.overflow, id);
+#ifndef GTAP_PHASE_TIMERS
+    atomicAdd(&S.st[GTAP_STAT_OVERFLOW_PUSHES], 1ull);
+#endif
+    (void)S;
+}
+
 // Allocate a child, write its header, stage it for this round's push.
-// Children are invisible to other workers until the round ends
-// (reference contract of __gtap_spawn_task).
+// Children are invisible to other workers until the task that spawned them
+// has filled their frames (reference contract of __gtap_spawn_task: the
+// caller writes the frame after this returns).
 __device__ __forceinline__ void* rt_spawn(const Arena& A, WarpShared& S, int kind, int q, int* child_count,
                                           int* out_tid, bool retain, bool detached) {
     const unsigned lane = lane_id();
@@ -319,23 +333,31 @@ __device__ __forceinline__ void* rt_spawn(const Arena& A, WarpShared& S, int kin
     *reinterpret_cast<int4*>(h) = hw;
     const unsigned m = __activemask();
     const int s = warp_agg_inc(&S.cnt[q], A.num_queues == 1 ? m : __match_any_sync(m, q));
+    bool charged = false;
     if (s < A.spawn_cap) {
         S.sbuf[q * A.spawn_cap + s] = id | (int)(lane << kIdBits);
     } else if (detached) {
-        // staging area full: a child that never notifies its parent can go
-        // straight to the global overflow queue (its record is written above)
+        // staging area full: a child that never notifies its parent goes to
+        // the global overflow queue instead.  Its creation is charged to its
+        // root at once (the round's own charge covers staged children only),
+        // and it is pushed when its frame is complete: at this lane's next
+        // spawn or when its task returns.  One child per lane waits, so any
+        // number of children fits.
         atomicSub(&S.cnt[q], 1);
-        fence_acq_rel();
-        ring_push_one(A.overflow, id);
-#ifndef GTAP_PHASE_TIMERS
-        atomicAdd(&S.st[GTAP_STAT_OVERFLOW_PUSHES], 1ull);
-#endif
+        const int r = S.l_root[lane];
+        red_add_relaxed(&A.outstanding[r], 1ll);
+        red_add_relaxed(reinterpret_cast<long long*>(&A.results[r].tasks), 1ll);
+        atomicAdd(&S.st[GTAP_STAT_TASKS], 1ull);
+        charged = true;
+        const int prev = S.l_pend[lane];
+        S.l_pend[lane] = id;
+        if (prev >= 0) push_overflow_child(A, S, prev);
     } else {
         GTAP_ERROR(A, ERR_SPAWN_BUFFER_OVERFLOW, S.l_tid[lane], q, s, A.spawn_cap);
     }
     if (child_count) ++*child_count;
     if (!detached) S.l_spawned[lane] += 1;
-    S.l_created[lane] += 1;
+    if (!charged) S.l_created[lane] += 1;
     return frame_of(A, id);
 }
 
@@ -783,12 +805,15 @@ static __device__ int admit(const Arena& A, WarpShared& S, int& my_tid) {
         }
 #endif
         int kind = Prog::root_kind(rd.kind);
+        bool valid = true;
         if (kind < 0) {
             GTAP_ERROR(A, ERR_INVALID_KIND, id, -1, rd.kind, GTAP_KIND_COUNT);
             kind = 0;
+            valid = false;
         } else if (!Prog::root_args_ok(rd)) {
             GTAP_ERROR(A, ERR_INVALID_ARGUMENT, id, -1, rd.kind, 0);
             kind = 0;
+            valid = false;
         }
         TaskHeader* h = hdr_of(A, id);
         int4 hw;
@@ -797,15 +822,19 @@ static __device__ int admit(const Arena& A, WarpShared& S, int& my_tid) {
         hw.z = 0;
         hw.w = slot;
         *reinterpret_cast<int4*>(h) = hw;
-        Prog::init_root(A, rd, frame_of(A, id));
+        if (valid) Prog::init_root(A, rd, frame_of(A, id));
         gtap_root_result* res = &A.results[slot];
+        // a serve-mode slot is reused after its previous root was polled:
+        // everything the root accumulates starts here
+        res->value = 0;
+        res->tasks = 1;   // the root itself; its descendants are added as they are created
+        res->t_done_ns = 0;
         res->t_admit_ns = global_ns();
         res->index = idx;
         res->status = GTAP_ROOT_RUNNING;
         // the root counts as one outstanding task from here on; its finish
         // enters this or another warp's balance like any other task
         atom_add_acq_rel(&A.outstanding[slot], 1ll);
-        red_add_relaxed(reinterpret_cast<long long*>(&res->tasks), 1ll);
         S.l_created[lane] = 0;
         S.l_root[lane] = slot;
         my_tid = id;
@@ -830,7 +859,22 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
     int last_victim = -1;
     int backoff = 0;
     bool having = false;
-    const unsigned long long t_start = global_ns();
+    // watchdog (lane 0): a batch launch is bounded as a whole; a serve
+    // session only while roots are outstanding and none completes
+    unsigned long long t_watch = global_ns();
+    unsigned seen_done = 0;
+    auto watchdog_expired = [&]() -> bool {
+        const unsigned long long now = global_ns();
+        if (A.mode == 2) {
+            const unsigned c = ld_relaxed(A.completed);
+            if (c != seen_done || c >= ld_relaxed(A.published)) {
+                seen_done = c;
+                t_watch = now;
+                return false;
+            }
+        }
+        return now - t_watch > A.watchdog_ns;
+    };
     int round = 0;
     int src_kind = 0;                        // debug builds: where this round's tasks came from
     bool idle = false;                       // counted in the hungry replicas
@@ -885,7 +929,7 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
                         unsigned pub = ld_acquire(A.published);
                         if (ld_acquire(A.completed) >= pub && ld_relaxed(A.next_root) >= pub) stop = 1;
                     }
-                    if (!stop && global_ns() - t_start > A.watchdog_ns) {
+                    if (!stop && watchdog_expired()) {
                         GTAP_ERROR(A, ERR_TIMEOUT, -1, -1, 0, 0);
                         stop = 1;
                     }
@@ -972,6 +1016,51 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
         const unsigned fin = __ballot_sync(0xffffffffu, active && (lane_flags & kLaneFinished));
         const bool my_fin = active && ((fin >> lane) & 1u);
         const unsigned spawners = __ballot_sync(0xffffffffu, active && S.l_spawned[lane] > 0);
+        // (0) the children this round created count for their roots before
+        //     any of them can be seen by another warp: one that ran and
+        //     finished elsewhere before its creation was counted could bring
+        //     its root's counter to zero early.  One leader per distinct root.
+        const int r0 = S.l_root[0];   // lane 0 always runs a task when nb > 0
+        const bool one_root = __all_sync(0xffffffffu, !active || S.l_root[lane] == r0);
+        const int my_root = active ? S.l_root[lane] : -1;
+        const unsigned grp = one_root ? 0xffffffffu : __match_any_sync(0xffffffffu, my_root);
+        {
+            const int created = active ? S.l_created[lane] : 0;
+            if (__any_sync(0xffffffffu, created != 0)) {
+                if (one_root) {
+                    const int c_sum = (int)__reduce_add_sync(0xffffffffu, (unsigned)created);
+                    if (lane == 0) account_root(A, S, r0, c_sum, 0);
+                } else {
+                    int c_sum = 0;
+                    if (active) c_sum = (int)__reduce_add_sync(grp, (unsigned)created);
+                    unsigned leaders = __ballot_sync(0xffffffffu, active && c_sum != 0 && (unsigned)__ffs(grp) - 1u == lane);
+                    while (leaders) {
+                        if (lane == (unsigned)__ffs(leaders) - 1u) account_root(A, S, my_root, c_sum, 0);
+                        __syncwarp();
+                        leaders &= leaders - 1u;
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        //     Detached children that did not fit the staging buffer and still
+        //     wait (one per lane, charged when spawned): their frames are
+        //     complete now that the task bodies returned.
+        {
+            const int pend = S.l_pend[lane];
+            const unsigned pm = __ballot_sync(0xffffffffu, pend >= 0);
+            if (pm) {
+                S.l_pend[lane] = -1;
+                fence_acq_rel();
+                __syncwarp();   // every lane's frame stores are ordered before any push
+                const int n = __popc(pm);
+                const int v = __shfl_sync(0xffffffffu, pend, (int)lane < n ? (int)__fns(pm, 0, (int)lane + 1) : 0);
+                ring_push_warp(A, A.overflow, v, n);
+#ifndef GTAP_PHASE_TIMERS
+                if (lane == 0) S.st[GTAP_STAT_OVERFLOW_PUSHES] += (unsigned long long)n;
+#endif
+            }
+        }
         // (1) orphans: children of tasks that returned without a taskwait
         if (fin & spawners) {
             for (int q = 0; q < A.num_queues; ++q) {
@@ -1129,33 +1218,26 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
         }
         GTAP_PHASE_MARK(ph4);
         GTAP_PHASE_ADD(13, ph3b, ph4);
-        // (6) per-root accounting, one leader per distinct root
-        const int r0 = S.l_root[0];   // lane 0 always runs a task when nb > 0
-        if (__all_sync(0xffffffffu, !active || S.l_root[lane] == r0)) {
+        // (6) per-root accounting of finishes and values (creations were
+        //     charged in (0)), one leader per distinct root
+        if (one_root) {
             // every task of the round belongs to one root: warp sums, lane 0 books them
-            const unsigned created = active ? (unsigned)S.l_created[lane] : 0u;
             const unsigned value = active ? (unsigned)S.l_value[lane] : 0u;
-            const int c_sum = (int)__reduce_add_sync(0xffffffffu, created);
             const int f_sum = __popc(fin);
             const int v_sum = (int)__reduce_add_sync(0xffffffffu, value);
             if (lane == 0) {
                 if (v_sum) atomicAdd(reinterpret_cast<unsigned long long*>(&A.results[r0].value),
                                      (unsigned long long)(long long)v_sum);
-                account_root(A, S, r0, c_sum, f_sum);
+                account_root(A, S, r0, 0, f_sum);
                 if (S.nbal > 1) age_bal(A, S);
                 else S.bal[0].touched = 0;
             }
             __syncwarp();
         } else {
-            const int created = active ? S.l_created[lane] : 0;
-            const int finished = my_fin ? 1 : 0;
             const int value = active ? S.l_value[lane] : 0;
-            const int r = active ? S.l_root[lane] : -1;
-            unsigned grp = __match_any_sync(0xffffffffu, r);
-            int c_sum = created, f_sum = finished, v_sum = value;
+            int f_sum = 0, v_sum = 0;
             if (active) {
-                c_sum = (int)__reduce_add_sync(grp, (unsigned)created);
-                f_sum = (int)__reduce_add_sync(grp, (unsigned)finished);
+                f_sum = __popc(fin & grp);
                 v_sum = (int)__reduce_add_sync(grp, (unsigned)value);
             }
             const bool leader = active && ((unsigned)__ffs(grp) - 1u == lane);
@@ -1164,9 +1246,9 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
             while (leaders) {
                 const unsigned l = (unsigned)__ffs(leaders) - 1u;
                 if (lane == l) {
-                    if (v_sum) atomicAdd(reinterpret_cast<unsigned long long*>(&A.results[r].value),
+                    if (v_sum) atomicAdd(reinterpret_cast<unsigned long long*>(&A.results[my_root].value),
                                          (unsigned long long)(long long)v_sum);
-                    account_root(A, S, r, c_sum, f_sum);
+                    account_root(A, S, my_root, 0, f_sum);
                 }
                 __syncwarp();
                 leaders &= leaders - 1u;
@@ -1197,7 +1279,7 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
             int stop = 0;
             if (lane == 0) {
                 if (aborted(A)) stop = 1;
-                else if (global_ns() - t_start > A.watchdog_ns) {
+                else if (watchdog_expired()) {
                     GTAP_ERROR(A, ERR_TIMEOUT, -1, -1, 1, 0);
                     stop = 1;
                 }
@@ -1232,6 +1314,7 @@ __device__ __forceinline__ void thread_worker_run(const Arena& A, WarpShared& S,
     // first ids come from the private range
     const int first = min(64, A.ids_per_worker);
     const int range = A.id_base + worker * A.ids_per_worker;
+    S.l_pend[lane] = -1;
     if ((int)lane < first) S.avail[lane] = range + (int)lane;
     if ((int)lane + 32 < first) S.avail[lane + 32] = range + (int)lane + 32;
     if (lane == 0) {

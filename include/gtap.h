@@ -69,7 +69,8 @@ int gtap_serve_start(int32_t ring_capacity, int32_t admit_watermark);
 int gtap_serve_enqueue(const gtap_root* roots, int32_t n, int32_t* first_index);
 /* Poll completions: writes up to max finished root indices, returns count via *n_out. */
 int gtap_serve_poll(int32_t* indices, int32_t max, int32_t* n_out);
-/* Read results of finished roots (by index). */
+/* Read results of finished roots by ring slot: during the session, and after
+ * gtap_serve_shutdown until the next session or launch. */
 int gtap_serve_results(const int32_t* indices, int32_t n, gtap_root_result* out);
 /* Drain outstanding roots, stop the kernel, return its statistics. */
 int gtap_serve_shutdown(gtap_run_stats* stats);

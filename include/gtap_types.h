@@ -80,7 +80,8 @@ typedef struct gtap_config {
     int64_t total_ids;       /* task records in the arena (<= 2^27) */
     int32_t frame_bytes;     /* largest task frame in bytes (__gtap_auto_task_data_size) */
     int32_t admit_batch;     /* roots an idle worker claims at once */
-    int64_t watchdog_ms;     /* hard wall-clock limit per launch; the kernel returns GTAP_ERROR_TIMEOUT */
+    int64_t watchdog_ms;     /* hard wall-clock limit per launch (serve mode: per stretch with roots
+                                outstanding and none completing); the kernel returns GTAP_ERROR_TIMEOUT */
     int32_t profile_samples; /* per-worker timeline samples, 0 = off (MAX_PROFILE_DATA) */
     int32_t result_handles;  /* legacy result-handle table capacity (GTAP_RESULT_HANDLE_CAPACITY) */
     int32_t publish_lazy;    /* 0: publish every task beyond the next batch each round (reference push_batch);
