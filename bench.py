@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-per-root", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--serve-roots", type=int, default=200,
+                    help="roots per serve session (BFS on R-MAT 16-20 / tree sums 2^18-2^20); 0 = no serve run")
     ap.add_argument("--config", default="", help="json dict of gtap_config overrides (applied last)")
     ap.add_argument("--tuned", default=TUNED, help="autotuner result whose overrides are applied first ('' = none)")
     return ap.parse_args()
@@ -331,6 +333,23 @@ def main():
                     "kernel_ms_sum": st_pr.kernel_ms, "results_match": ok_pr, "config": "library defaults",
                     "speedup_batched_vs_per_root": value / world / (sum(r.tasks for r in res_pr) / pr_s)}
 
+    # serve mode: capacity, then Poisson arrivals at fractions of it and at
+    # 2000 roots/s (the lowest served rate asked for), library defaults
+    serve = None
+    if args.serve_roots > 0:
+        gt.gtap_finalize()
+        from gtap_b200 import serve_bench
+        sv = serve_bench.run(loads=(0.5, 0.9), rates=(2000,), count=args.serve_roots)
+        keys = ("load", "rate_roots_per_s", "throughput_roots_per_s", "tasks_per_s", "latency_ms",
+                "device_service_ms", "ok")
+        serve = {"workload": "50% async BFS on R-MAT scale 16-20 (edge factor 16), 50% int64 tree sums over "
+                             "2^18-2^20-node unbalanced binary trees; Poisson arrivals",
+                 "roots_per_session": args.serve_roots, "config": "library defaults",
+                 "capacity_roots_per_s": sv["capacity"]["throughput_roots_per_s"],
+                 "capacity_tasks_per_s": sv["capacity"]["tasks_per_s"],
+                 "sessions": [{k: r[k] for k in keys} for r in [sv["capacity"]] + sv["sessions"]],
+                 "ok": sv["capacity"]["ok"] and all(r["ok"] for r in sv["sessions"])}
+
     cpu = None
     if not args.no_cpu and rank == 0 and world == 1:
         tasks_gpu = [r.tasks for r in res]
@@ -347,7 +366,7 @@ def main():
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "runtime": {k: v for k, v in cfg.as_dict().items()}, "tuned_from": tuned_from},
             "verified": verified, "gpu_launches": 2 * args.steps, "e2e": e2e, "roofline": roof,
-            "cpu_baseline": cpu, "per_root_launch": per_root, "clocks": ck,
+            "cpu_baseline": cpu, "per_root_launch": per_root, "serve": serve, "clocks": ck,
             "scheduler": {"steal_success_rate": counters.get("steal_successes", 0) /
                           max(1, counters.get("steal_attempts", 0)),
                           "idle_polls": counters.get("idle_polls", 0),

@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "../../include/gtap.h"
+#include "gtap_block_programs.cuh"
 #include "gtap_programs.cuh"
 #include "gtap_selftest.cuh"
 
@@ -42,7 +43,9 @@ struct Runtime {
     int workers = 0;            // arena capacity: max over the kernel variants
     int workers_full = 0;       // thread_worker_kernel<BuiltinProgram>
     int workers_light = 0;      // thread_worker_kernel_lb<BuiltinProgramLight>
+    int workers_block = 0;      // block_worker_kernel<BlockProgram>: one worker per block (block mode only)
     int last_workers = 0;       // workers of the last launch
+    bool last_block = false;    // the last launch ran the block kernel
     int external_workers = 0;   // workers of a kernel the caller launches (drop-in header), 0 = none
     int warps_per_block = 0;
     size_t smem_bytes = 0;
@@ -149,8 +152,16 @@ bool roots_need_sorts(const gtap_root* roots, int n) {
     return false;
 }
 
+constexpr size_t kBlockSmemBytes = (size_t)BlockProgram::kSmemInts * sizeof(int);
+
+bool block_mode() { return g.cfg.mode == GTAP_MODE_BLOCK; }
+
 // launch the worker kernel variant; A.num_workers must match it
 cudaError_t launch_worker(const Arena& A, bool light, cudaStream_t s) {
+    if (block_mode()) {
+        block_worker_kernel<BlockProgram><<<A.num_workers, g.cfg.block, kBlockSmemBytes, s>>>(A);
+        return cudaGetLastError();
+    }
     const int blocks = A.num_workers / g.warps_per_block;
     const bool one = g.cfg.num_queues == 1;
     if (light && one) thread_worker_kernel_lb<BuiltinProgramLight, 1><<<blocks, g.cfg.block, g.smem_bytes, s>>>(A);
@@ -357,7 +368,7 @@ int collect_stats(gtap_run_stats* stats) {
     for (int i = 0; i < GTAP_STAT_COUNT; ++i) stats->counters[i] = 0;
     for (int w = 0; w < W; ++w)
         for (int i = 0; i < GTAP_STAT_COUNT; ++i) stats->counters[i] += h[(size_t)w * GTAP_STAT_COUNT + i];
-    stats->grid = W / g.warps_per_block;
+    stats->grid = g.last_block ? W : W / g.warps_per_block;
     stats->block = g.cfg.block;
     stats->workers = W;
     return 0;
@@ -377,8 +388,9 @@ int launch_resident(int n_roots, cudaStream_t s, float* ms_out, bool light) {
     GT_CUDA(cudaMemsetAsync(g.dbg + 2 * g.cfg.total_ids, 0xFF,
                             (size_t)g.cfg.num_queues * g.workers * g.cfg.deque_capacity * sizeof(int), s));
 #endif
-    const int W = light ? g.workers_light : g.workers_full;
+    const int W = block_mode() ? g.workers_block : light ? g.workers_light : g.workers_full;
     g.last_workers = W;
+    g.last_block = block_mode();
     Arena A = make_arena(n_roots, 0, W);
     const int fresh_base = W * g.cfg.ids_per_worker;
     A.admit_watermark = admission_watermark(W);
@@ -484,10 +496,20 @@ static int initialize_impl(const gtap_config* cfg_in, int external_workers) {
     g.warps_per_block = c.block / 32;
     g.workers_light = grid_light * g.warps_per_block;
     g.workers_full = grid_full * g.warps_per_block;
-    g.workers = std::max(std::max(g.workers_light, g.workers_full), external_workers);
+    g.workers_block = 0;
+    if (c.mode == GTAP_MODE_BLOCK) {
+        // one worker per block; the grid fills the GPU unless capped
+        if (c.block > kBMaxThreads) return GTAP_ERROR_INVALID_ARGUMENT;
+        int per_sm_block = 0;
+        GT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_block, &block_worker_kernel<BlockProgram>, c.block,
+                                                              kBlockSmemBytes));
+        if (per_sm_block < 1) return GTAP_ERROR_INVALID_ARGUMENT;
+        g.workers_block = pick(per_sm_block);
+    }
+    g.workers = std::max(std::max(std::max(g.workers_light, g.workers_full), external_workers), g.workers_block);
     g.external_workers = external_workers;
     g.last_workers = g.workers_light;
-    if (c.grid == 0) c.grid = std::max(grid_light, grid_full);
+    if (c.grid == 0) c.grid = c.mode == GTAP_MODE_BLOCK ? g.workers_block : std::max(grid_light, grid_full);
     if ((long long)g.workers * c.ids_per_worker + 1 > c.total_ids) {
         // private ranges that would not fit may use at most half of the arena
         // (id 0 may be reserved for a caller-launched kernel's initial task)
@@ -587,6 +609,7 @@ int gtap_external_prepare(void* arena_out, int64_t arena_bytes) {
     if ((++g.epoch & 0xFFFFu) == 0) ++g.epoch;   // epoch 0 would match never-written ring slots
     const int W = g.external_workers;
     g.last_workers = W;
+    g.last_block = false;
     Arena A = make_arena(1, 0, W);
     A.id_base = 1;   // id 0 is the initial task's (its frame is __gtap_get_task_data(0))
     A.admit_watermark = 0;
@@ -685,7 +708,7 @@ int gtap_launch(const gtap_root* roots, int32_t n_roots, gtap_root_result* resul
     int rc = ensure_root_capacity(n_roots);
     if (rc) return rc;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    if (roots_need_sorts(roots, n_roots) && g.workers_full == 0) return GTAP_ERROR_INVALID_ARGUMENT;
+    if (!block_mode() && roots_need_sorts(roots, n_roots) && g.workers_full == 0) return GTAP_ERROR_INVALID_ARGUMENT;
     GT_CUDA(cudaMemcpyAsync(g.d_roots, roots, sizeof(gtap_root) * n_roots, cudaMemcpyHostToDevice, s));
     float ms = 0.f;
     int st = launch_resident(n_roots, s, &ms, !roots_need_sorts(roots, n_roots));
@@ -717,7 +740,7 @@ int gtap_launch_per_root(const gtap_root* roots, int32_t n_roots, gtap_root_resu
     for (int i = 0; i < n_roots && st == 0; ++i) {
         GT_CUDA(cudaMemcpyAsync(g.d_roots, roots + i, sizeof(gtap_root), cudaMemcpyHostToDevice, s));
         float ms = 0.f;
-        if (roots_need_sorts(roots + i, 1) && g.workers_full == 0) return GTAP_ERROR_INVALID_ARGUMENT;
+        if (!block_mode() && roots_need_sorts(roots + i, 1) && g.workers_full == 0) return GTAP_ERROR_INVALID_ARGUMENT;
         st = launch_resident(1, s, &ms, !roots_need_sorts(roots + i, 1));
         ms_total += ms;
         if (results) {
@@ -736,7 +759,7 @@ int gtap_launch_per_root(const gtap_root* roots, int32_t n_roots, gtap_root_resu
     if (stats) {
         *stats = total;
         stats->kernel_ms = ms_total;
-        stats->grid = g.last_workers / g.warps_per_block;
+        stats->grid = g.last_block ? g.last_workers : g.last_workers / g.warps_per_block;
         stats->block = g.cfg.block;
         stats->workers = g.last_workers;
         stats->status = st;
@@ -860,11 +883,14 @@ extern "C" int gtap_serve_start(int32_t ring_capacity, int32_t admit_watermark) 
     GT_CUDA(cudaEventCreate(&g.serve_ev1));
     if (g.h_report) memset(g.h_report, 0, sizeof(GtapErrorReport));
     if ((++g.epoch & 0xFFFFu) == 0) ++g.epoch;   // epoch 0 would match never-written ring slots
-    // serve mode runs the light kernel: fib, n-queens, BFS and tree roots
-    g.last_workers = g.workers_light;
-    Arena A = make_arena(ring_capacity, 2, g.workers_light);
-    A.admit_watermark = admit_watermark > 0 ? admit_watermark : admission_watermark(g.workers_light);
-    reset_kernel<<<64, 256, 0, g.serve_stream>>>(A, g.counters, ring_capacity, g.workers_light * g.cfg.ids_per_worker);
+    // serve mode runs the light kernel (fib, n-queens, BFS and tree roots), or
+    // the block kernel in block mode (every kind)
+    const int W = block_mode() ? g.workers_block : g.workers_light;
+    g.last_workers = W;
+    g.last_block = block_mode();
+    Arena A = make_arena(ring_capacity, 2, W);
+    A.admit_watermark = admit_watermark > 0 ? admit_watermark : admission_watermark(W);
+    reset_kernel<<<64, 256, 0, g.serve_stream>>>(A, g.counters, ring_capacity, W * g.cfg.ids_per_worker);
     GT_CUDA(cudaGetLastError());
     GT_CUDA(cudaEventRecord(g.serve_ev0, g.serve_stream));
     GT_CUDA(launch_worker(A, true, g.serve_stream));

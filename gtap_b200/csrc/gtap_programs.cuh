@@ -704,14 +704,20 @@ struct BuiltinProgramT {
     // Argument ranges the built-in tasks rely on: fib's serial leaf handles
     // n <= 64, n-queens packs n and the cutoff into 8 bits with n <= 32
     // columns; the array kinds need their arrays, a count that fits int32 and
-    // a start node inside it.  A root that fails is recorded as an error and
-    // touches none of its arrays.
+    // a start node inside it.  The recursions end only with a sort cutoff of
+    // at least 2 (a one-key cilksort splits into 0, 0, 0 and 1 keys again) and
+    // a merge cutoff of at least 3 (a merge of one key with one key splits
+    // into itself).  A root that fails is recorded as an error and touches
+    // none of its arrays.
     __device__ static bool root_args_ok(const gtap_root& rd) {
         switch (rd.kind) {
             case GTAP_KIND_FIB: return rd.i0 <= 64;
             case GTAP_KIND_NQ: return rd.i0 >= 0 && rd.i0 <= 32 && rd.i1 >= 0 && rd.i1 < 256;
             case GTAP_KIND_CILKSORT:
+                if (rd.i0 < 2 || rd.i1 < 3) return false;
+                return rd.n >= 0 && rd.n <= 0x7FFFFFFF && (rd.n == 0 || (rd.p0 && rd.p1 && rd.p2));
             case GTAP_KIND_MERGESORT:
+                if (rd.i1 < 3) return false;
                 return rd.n >= 0 && rd.n <= 0x7FFFFFFF && (rd.n == 0 || (rd.p0 && rd.p1 && rd.p2));
             case GTAP_KIND_BFS:
                 return rd.p0 && rd.p1 && rd.p2 && rd.n > 0 && rd.n <= 0x7FFFFFFF && rd.i0 >= 0 && rd.i0 < rd.n;

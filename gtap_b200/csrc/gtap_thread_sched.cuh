@@ -99,6 +99,8 @@ struct WarpShared {
     unsigned long long st[GTAP_STAT_COUNT];
     int worker;
     int prof_h, prof_w;
+    unsigned seen_done;        // watchdog (lane 0): completions seen at t_watch
+    unsigned long long t_watch;
     int* sbuf;                 // [num_queues][spawn_cap] staged child ids (| spawner lane << 27)
     int* lstk;                 // [num_queues][kLocalCap] ready tasks not yet visible to thieves
 };
@@ -861,19 +863,21 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
     bool having = false;
     // watchdog (lane 0): a batch launch is bounded as a whole; a serve
     // session only while roots are outstanding and none completes
-    unsigned long long t_watch = global_ns();
-    unsigned seen_done = 0;
+    if (lane == 0) {
+        S.t_watch = global_ns();
+        S.seen_done = 0;
+    }
     auto watchdog_expired = [&]() -> bool {
         const unsigned long long now = global_ns();
         if (A.mode == 2) {
             const unsigned c = ld_relaxed(A.completed);
-            if (c != seen_done || c >= ld_relaxed(A.published)) {
-                seen_done = c;
-                t_watch = now;
+            if (c != S.seen_done || c >= ld_relaxed(A.published)) {
+                S.seen_done = c;
+                S.t_watch = now;
                 return false;
             }
         }
-        return now - t_watch > A.watchdog_ns;
+        return now - S.t_watch > A.watchdog_ns;
     };
     int round = 0;
     int src_kind = 0;                        // debug builds: where this round's tasks came from

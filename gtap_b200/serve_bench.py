@@ -13,11 +13,16 @@ completion ring between arrivals, and records
                    (includes the wait for admission when the GPU is saturated)
   device service   the kernel's own stamps, admission -> last task finished
 
+The capacity of the GPU for this workload is measured first, with every root
+of a session enqueued at once; then sessions run at fixed fractions of that
+capacity (where latency means something) and at the requested absolute rates
+(above capacity they measure queueing).
+
 All device buffers (graphs, trees, one BFS depth array per BFS root) exist
 before the session starts: while the persistent kernel holds the SMs no other
 kernel may be launched.
 
-    python -m gtap_b200.serve_bench --rates 2000,5000,10000,20000,50000
+    python -m gtap_b200.serve_bench --loads 0.25,0.5,0.75,0.9 --rates 2000,50000
 """
 import argparse
 import json
@@ -44,6 +49,7 @@ class ServeWorkload:
             self.trees.append({"n": n, "arrays": [torch.from_numpy(a).cuda() for a in (left, right, value, size)],
                                "sum": int(value.astype(np.int64).sum())})
         self.rng = np.random.default_rng(seed)
+        self.ref_depth = {}   # graph index -> a validated depth array
 
     def draw(self, count):
         """(kind, index) per root: kind 0 = BFS on graph index, 1 = tree sum."""
@@ -94,12 +100,15 @@ def pct(x, q):
     return float(np.percentile(np.asarray(x), q)) if len(x) else None
 
 
-def run_rate(gt, wl, rate, count, seed=11):
-    """One serve session at `rate` roots/s for `count` roots."""
+def run_rate(gt, wl, rate, count, seed=11, limit_s=120.0):
+    """One serve session of `count` roots at `rate` roots/s (None: all at once)."""
     plan = wl.draw(count)
     roots, depths = wl.roots(plan)
-    rng = np.random.default_rng(seed + int(rate))
-    arrivals = np.cumsum(rng.exponential(1.0 / rate, count))
+    if rate is None:
+        arrivals = np.zeros(count)
+    else:
+        rng = np.random.default_rng(seed + int(rate))
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, count))
     gt.serve_start(ring_capacity=max(64, count))
     slot_of = {}
     done_t = {}
@@ -116,8 +125,8 @@ def run_rate(gt, wl, rate, count, seed=11):
                 nxt = end
             for s in gt.serve_poll(4096):
                 done_t[slot_of[s]] = time.perf_counter() - t0
-            if now > 60.0:
-                raise RuntimeError("serve run at %d roots/s did not finish in 60 s" % rate)
+            if now > limit_s:
+                raise RuntimeError("serve run at %s roots/s did not finish in %.0f s" % (rate, limit_s))
         wall = time.perf_counter() - t0
     finally:
         st = gt.serve_shutdown()
@@ -132,30 +141,55 @@ def run_rate(gt, wl, rate, count, seed=11):
         if kind == 1:
             ok &= by_root[j].value == wl.trees[i]["sum"]
     return {"rate_roots_per_s": rate, "roots": count, "wall_s": wall, "ok": bool(ok) and st.status == 0,
+            "tasks": tasks,
             "throughput_roots_per_s": count / wall, "tasks_per_s": tasks / wall,
             "latency_ms": {"p50": pct(lat, 50), "p99": pct(lat, 99), "max": max(lat)},
             "device_service_ms": {"p50": pct(svc, 50), "p99": pct(svc, 99)}, "depth_arrays": depths}
 
 
-def run(rates, count, config=None, check_bfs=2):
+def _check_depths(wl, r):
+    """Every BFS root's depths: BFS distances are unique, so the first array
+    seen for a graph is validated as a distance labelling and the others
+    must equal it."""
+    import torch
+    for d in r.pop("depth_arrays"):
+        if d is None:
+            continue
+        gi = next(i for i, g in enumerate(wl.graphs) if g["nv"] == d.numel())
+        ref = wl.ref_depth.get(gi)
+        if ref is None:
+            g = wl.graphs[gi]
+            if bfs_depths_valid(g["row"].cpu().numpy(), g["col"].cpu().numpy(), g["src"], d.cpu().numpy()):
+                wl.ref_depth[gi] = d.clone()
+            else:
+                r["ok"] = False
+        elif not torch.equal(d, ref):
+            r["ok"] = False
+    return r
+
+
+def run(loads=(0.25, 0.5, 0.75, 0.9), rates=(), count=300, config=None, workload=None):
+    """Capacity session, then one session per load fraction and per absolute
+    rate.  Returns {"capacity": {...}, "sessions": [...]}."""
     import torch
     import gtap_b200 as gt
     torch.cuda.init()
-    wl = ServeWorkload(gt)
+    wl = workload or ServeWorkload(gt)
     gt.gtap_initialize(gt.default_config(**(config or {})))
-    out = []
+    out = {"sessions": []}
     try:
+        cap = _check_depths(wl, run_rate(gt, wl, None, count))
+        cap["load"] = None
+        out["capacity"] = cap
+        capacity = cap["throughput_roots_per_s"]
+        for f in loads:
+            r = _check_depths(wl, run_rate(gt, wl, f * capacity, count))
+            r["load"] = f
+            out["sessions"].append(r)
         for rate in rates:
-            r = run_rate(gt, wl, rate, count)
-            # a few BFS depth arrays are validated as distance labellings
-            checked = 0
-            for d in r.pop("depth_arrays"):
-                if d is None or checked >= check_bfs:
-                    continue
-                g = next(g for g in wl.graphs if g["nv"] == d.numel())
-                r["ok"] &= bfs_depths_valid(g["row"].cpu().numpy(), g["col"].cpu().numpy(), g["src"], d.cpu().numpy())
-                checked += 1
-            out.append(r)
+            r = _check_depths(wl, run_rate(gt, wl, rate, count))
+            r["load"] = rate / capacity
+            out["sessions"].append(r)
     finally:
         gt.gtap_finalize()
     return out
@@ -163,11 +197,17 @@ def run(rates, count, config=None, check_bfs=2):
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    ap.add_argument("--rates", default="2000,5000,10000,20000,50000")
-    ap.add_argument("--roots", type=int, default=1000, help="roots per rate")
+    ap.add_argument("--loads", default="0.25,0.5,0.75,0.9", help="fractions of the measured capacity")
+    ap.add_argument("--rates", default="2000,50000", help="absolute arrival rates, roots/s")
+    ap.add_argument("--roots", type=int, default=300, help="roots per session")
     a = ap.parse_args(argv)
-    for r in run([int(x) for x in a.rates.split(",")], a.roots):
+    loads = [float(x) for x in a.loads.split(",") if x]
+    rates = [int(x) for x in a.rates.split(",") if x]
+    out = run(loads, rates, a.roots)
+    print(json.dumps(out["capacity"]), flush=True)
+    for r in out["sessions"]:
         print(json.dumps(r), flush=True)
+    return 0 if out["capacity"]["ok"] and all(r["ok"] for r in out["sessions"]) else 1
 
 
 if __name__ == "__main__":
