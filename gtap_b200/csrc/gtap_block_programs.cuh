@@ -24,8 +24,8 @@ using prog::K_MERGESORT;
 using prog::K_NQ;
 using prog::K_TREESUM;
 
-constexpr int kLeafMax = 4096;             // keys one leaf sort or merge stages in shared memory
-constexpr int kSmemInts = 2 * kLeafMax;    // dynamic shared memory of the block kernel (32 KB)
+constexpr int kLeafMax = 2048;             // keys one leaf sort or merge stages in shared memory
+constexpr int kSmemInts = 2 * kLeafMax;    // dynamic shared memory of the block kernel (16 KB)
 
 __device__ __forceinline__ void* ptr_of(int lo, int hi) {
     return reinterpret_cast<void*>((unsigned long long)(unsigned)lo | ((unsigned long long)(unsigned)hi << 32));

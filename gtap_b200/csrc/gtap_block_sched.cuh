@@ -28,10 +28,12 @@
 
 namespace gtap {
 
-constexpr int kBStage = 1024;        // children staged per execution in shared memory
+constexpr int kBStage = 512;         // children staged per execution in shared memory
 constexpr int kBAvail = 256;         // free ids cached per block
 constexpr int kBAvailLow = 96;       // refill below this many
 constexpr int kBMaxThreads = 512;    // threads per block in block mode (a leaf task's width)
+constexpr int kBBal = 4;             // roots with a pre-charged balance per block
+constexpr int kBChunk = 256;         // credit taken from a root's counter at a time
 
 struct BlockShared {
     // the task this execution runs (written by warp 0 before the body)
@@ -54,7 +56,12 @@ struct BlockShared {
     int staged[kBStage];
     int pend[kBMaxThreads];          // per thread: a detached child past kBStage whose frame is being written
     unsigned long long st[GTAP_STAT_COUNT];
-    int scratch[32];                 // broadcasts of the task bodies
+    // pre-charged balances: the block holds credit[i] units of root bal_root[i]'s
+    // outstanding count; finishes add to it, creations draw on it
+    int nbal;
+    int bal_root[kBBal];
+    int bal_touched[kBBal];
+    long long bal_credit[kBBal];
 };
 
 // ---------------------------------------------------------------------------
@@ -180,6 +187,60 @@ __device__ __forceinline__ void bt_return_i32(const Arena& A, const BlockShared&
 // Any thread: add to the root's value (n-queens counts).
 __device__ __forceinline__ void bt_add_value(BlockShared& S, long long v) {
     atomicAdd(reinterpret_cast<unsigned long long*>(&S.value), (unsigned long long)v);
+}
+
+// ---------------------------------------------------------------------------
+// per-root balances (lane 0 of warp 0).  A root's counter = its live tasks +
+// the credit blocks hold for it, so it reaches zero exactly when the last task
+// has finished and every block has returned its credit; the global counter is
+// touched once per kBChunk creations and once per flush instead of per task.
+// ---------------------------------------------------------------------------
+static __device__ void bt_bal_flush(const Arena& A, BlockShared& S, int i) {
+    const long long c = S.bal_credit[i];
+    const int r = S.bal_root[i];
+    --S.nbal;
+    S.bal_root[i] = S.bal_root[S.nbal];
+    S.bal_credit[i] = S.bal_credit[S.nbal];
+    S.bal_touched[i] = S.bal_touched[S.nbal];
+    if (c != 0) outstanding_add(A, r, -c);
+}
+static __device__ int bt_bal_slot(const Arena& A, BlockShared& S, int r) {
+    for (int i = 0; i < S.nbal; ++i)
+        if (S.bal_root[i] == r) return i;
+    if (S.nbal == kBBal) bt_bal_flush(A, S, 0);
+    const int i = S.nbal++;
+    S.bal_root[i] = r;
+    S.bal_credit[i] = 0;
+    S.bal_touched[i] = 0;
+    return i;
+}
+// n creations for root r, before any of them is published
+static __device__ void bt_charge(const Arena& A, BlockShared& S, int r, int n) {
+    const int i = bt_bal_slot(A, S, r);
+    S.bal_touched[i] = 1;
+    long long c = S.bal_credit[i] - n;
+    if (c < 0) {
+        red_add_relaxed(&A.outstanding[r], (long long)kBChunk - c);
+        c = kBChunk;
+    }
+    S.bal_credit[i] = c;
+}
+// one finish of root r
+static __device__ void bt_credit(const Arena& A, BlockShared& S, int r) {
+    const int i = bt_bal_slot(A, S, r);
+    S.bal_touched[i] = 1;
+    S.bal_credit[i] += 1;
+}
+// after a task: balances of roots this task did not touch go back, so that
+// completions are not held up by blocks busy elsewhere
+static __device__ void bt_bal_age(const Arena& A, BlockShared& S) {
+    for (int i = S.nbal - 1; i >= 0; --i) {
+        if (S.bal_touched[i]) S.bal_touched[i] = 0;
+        else bt_bal_flush(A, S, i);
+    }
+}
+static __device__ void bt_bal_flush_all(const Arena& A, BlockShared& S) {
+    while (S.nbal > 0) bt_bal_flush(A, S, S.nbal - 1);
 }
 
 // ---------------------------------------------------------------------------
@@ -361,7 +422,7 @@ static __device__ void bt_round_end(const Arena& A, BlockShared& S) {
         if (S.value) atomicAdd(reinterpret_cast<unsigned long long*>(&A.results[root].value),
                                (unsigned long long)S.value);
         if (n_st > 0) {
-            red_add_relaxed(&A.outstanding[root], (long long)n_st);
+            bt_charge(A, S, root, n_st);
             red_add_relaxed(reinterpret_cast<long long*>(&A.results[root].tasks), (long long)n_st);
             S.st[GTAP_STAT_TASKS] += (unsigned long long)n_st;
         }
@@ -430,8 +491,9 @@ static __device__ void bt_round_end(const Arena& A, BlockShared& S) {
                     ring_push_one(A.idpool, t);
                 }
             }
-            outstanding_add(A, root, -1ll);
+            bt_credit(A, S, root);
         }
+        bt_bal_age(A, S);
         S.next = next;
         S.st[GTAP_STAT_EXECUTIONS] += 1;
         S.st[GTAP_STAT_ROUNDS] += 1;
@@ -456,6 +518,7 @@ __device__ void block_worker(const Arena& A, BlockShared& S, int* smem) {
         S.bump = A.id_base + blockIdx.x * A.ids_per_worker;
         S.bump_end = S.bump + A.ids_per_worker;
         S.avail_n = 0;
+        S.nbal = 0;
         for (int i = 0; i < GTAP_STAT_COUNT; ++i) S.st[i] = 0;
     }
     for (int i = tid; i < kBMaxThreads; i += blockDim.x) S.pend[i] = -1;
@@ -492,6 +555,7 @@ __device__ void block_worker(const Arena& A, BlockShared& S, int* smem) {
                 int stop = 0;
                 if (t < 0) {
                     S.st[GTAP_STAT_IDLE_POLLS] += 1;
+                    bt_bal_flush_all(A, S);
                     if (ld_acquire(A.done_flag) != 0 || aborted(A)) stop = 1;
                     if (A.mode == 2 && ld_relaxed(A.shutdown) != 0) {
                         const unsigned pub = ld_acquire(A.published);
@@ -569,6 +633,7 @@ __device__ void block_worker(const Arena& A, BlockShared& S, int* smem) {
         __syncthreads();
     }
     __syncthreads();
+    if (tid == 0) bt_bal_flush_all(A, S);
     if (w0 && (int)lane < GTAP_STAT_COUNT) A.stats[(size_t)S.worker * GTAP_STAT_COUNT + lane] = S.st[lane];
 }
 

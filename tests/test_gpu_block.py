@@ -55,7 +55,7 @@ def test_cilksort_cutoffs_2048(blk, n):
     sort_case(orc.keys(n, n), 2048, 2048)
 
 
-@pytest.mark.parametrize("n,sc,mc", [(50000, 64, 256), (77777, 4097, 4097), (1 << 16, 2, 3), (9999, 513, 3000)])
+@pytest.mark.parametrize("n,sc,mc", [(50000, 64, 256), (77777, 2049, 2049), (1 << 16, 2, 3), (9999, 513, 2000)])
 def test_cilksort_other_cutoffs(blk, n, sc, mc):
     sort_case(orc.keys(3 * n + 1, n), sc, mc)
 
@@ -68,7 +68,7 @@ def test_cilksort_duplicate_heavy_keys(blk):
     sort_case(keys, 2048, 2048)
 
 
-@pytest.mark.parametrize("n,cutoff", [(1, 128), (1000, 128), (1 << 16, 2048), (77777, 4096)])
+@pytest.mark.parametrize("n,cutoff", [(1, 128), (1000, 128), (1 << 16, 2048), (77777, 2048)])
 def test_mergesort(blk, n, cutoff):
     import torch
     keys = orc.keys(11 + n, n)
@@ -152,7 +152,7 @@ def test_cutoffs_that_never_end_are_rejected(blk, sc, mc):
 
 
 def test_leaf_cutoff_above_shared_memory_is_rejected(blk):
-    # a leaf of more than 4096 keys does not fit the block's staging buffers
+    # a leaf of more than 2048 keys does not fit the block's staging buffers
     import torch
     src = dev(orc.keys(1, 10000))
     arr = torch.empty_like(src)
