@@ -41,7 +41,7 @@ ERROR_INVALID_ARGUMENT = 11
 ERROR_NOT_INITIALIZED = 12
 
 STAT_NAMES = ["tasks", "executions", "rounds", "steal_attempts", "steal_successes", "stolen_tasks", "pops",
-              "published", "idle_polls", "overflow_pushes"]
+              "published", "idle_polls", "overflow_pushes", "join_finishes"]
 STAT_COUNT = 16
 
 

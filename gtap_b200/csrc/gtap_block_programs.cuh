@@ -170,7 +170,7 @@ __device__ void cilkmerge_task(const Arena& A, BlockShared& S, int* smem) {
         spawn_merge(A, S, a, as, b, bs, dst);
         spawn_merge(A, S, a + as, alen - as, b + bs, blen - bs, dst + as + bs);
     }
-    if (bt_join(A, S, 1)) return;
+    if (bt_join(A, S, 1, true)) return;
     bt_finish(S);
 }
 
@@ -210,7 +210,7 @@ __device__ void cilksort_task(const Arena& A, BlockShared& S, int* smem) {
     }
     if (st == 2) {
         if (threadIdx.x == 0) spawn_merge(A, S, tmp, len12, tmp + len12, len34, arr);
-        if (bt_join(A, S, 3)) return;
+        if (bt_join(A, S, 3, true)) return;
         st = 3;
     }
     if (st != 3 && threadIdx.x == 0) GTAP_ERROR(A, ERR_INVALID_TASKWAIT, S.task, -1, st, 3);
@@ -250,7 +250,7 @@ __device__ void mergesort_task(const Arena& A, BlockShared& S, int* smem) {
     }
     if (st == 1) {
         if (threadIdx.x == 0) spawn_merge(A, S, tmp, nl, tmp + nl, n - nl, out);
-        if (bt_join(A, S, 2)) return;
+        if (bt_join(A, S, 2, true)) return;
         st = 2;
     }
     if (st != 2 && threadIdx.x == 0) GTAP_ERROR(A, ERR_INVALID_TASKWAIT, S.task, -1, st, 2);

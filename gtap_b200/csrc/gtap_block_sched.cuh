@@ -46,6 +46,7 @@ struct BlockShared {
     int finished;
     long long value;                 // contributions to the root's value
     int next;                        // task to run next (continuation first), -1 none
+    int pre_task;                    // the task whose record round end already loaded into the fields above
     int stop;
     int worker;
     // id cache
@@ -150,8 +151,10 @@ __device__ __forceinline__ void* bt_spawn(const Arena& A, BlockShared& S, int ki
 
 // All threads (block-uniform).  taskwait: the children spawned since the last
 // one become this task's join count; true if the task must suspend.  The
-// header is written before any of the children is published.
-__device__ __forceinline__ bool bt_join(const Arena& A, BlockShared& S, int next_state) {
+// header is written before any of the children is published.  then_finish:
+// the task's code after this taskwait only finishes, so the block that
+// completes the join books the finish instead of running the task again.
+__device__ __forceinline__ bool bt_join(const Arena& A, BlockShared& S, int next_state, bool then_finish = false) {
     __syncthreads();
     const int n = S.spawned;
     __syncthreads();
@@ -161,6 +164,7 @@ __device__ __forceinline__ bool bt_join(const Arena& A, BlockShared& S, int next
         if (n > 0) {
             TaskHeader* h = hdr_of(A, S.task);
             h->state = (uint16_t)next_state;
+            if (then_finish) h->flags = (uint8_t)(S.flags | kFlagJoinFinish);
             h->join = n & kJoinCountMask;
             S.suspended = 1;
         }
@@ -408,6 +412,14 @@ static __device__ void bt_refill_ids(const Arena& A, BlockShared& S) {
     __syncwarp();
 }
 
+// lane 0: a finished task's id goes back to the cache (or the recycled-id
+// ring) unless its parent still reads the task's frame
+static __device__ void bt_release_id(const Arena& A, BlockShared& S, int id, unsigned flags) {
+    if (flags & kFlagRetain) return;
+    if (S.avail_n < kBAvail && S.avail_n >= 0) S.avail[S.avail_n++] = id;
+    else ring_push_one(A.idpool, id);
+}
+
 // Warp 0, after the body: charge, publish, join, finish, release.
 template <class Prog>
 static __device__ void bt_round_end(const Arena& A, BlockShared& S) {
@@ -416,6 +428,12 @@ static __device__ void bt_round_end(const Arena& A, BlockShared& S) {
     const int root = S.root;
     const int n_st = min(S.nstaged, kBStage);
     const bool finished = S.finished != 0 || S.suspended == 0;
+    // the newest child usually runs next on this block: lanes 1-3 load its
+    // record now, overlapping the fence and the join below (this block wrote
+    // it, before the barrier that precedes round end)
+    const int kept = n_st > 0 ? S.staged[n_st - 1] : -1;
+    int4 pre = make_int4(0, 0, 0, 0);
+    if (kept >= 0 && lane >= 1 && lane <= 3) pre = ld_data_v4(A.records + (size_t)kept * A.rec_stride + 16 * (lane - 1));
     // (1) the round's value and its children count for the root before any
     //     child can be seen by another block
     if (lane == 0) {
@@ -466,37 +484,65 @@ static __device__ void bt_round_end(const Arena& A, BlockShared& S) {
             red_add_relaxed(c, (unsigned long long)direct << kPosBits);
             S.st[GTAP_STAT_PUBLISHED] += (unsigned long long)direct;
         }
-        int next = keep ? S.staged[n_st - 1] : -1;
+        int next = kept;
         if (finished) {
-            // (4) join: the last child resumes its parent on this block
-            const int parent = S.parent;
-            if (parent >= 0) {
-                const int old = atom_add_acquire(&hdr_of(A, parent)->join, -1);
-                if ((old & kJoinCountMask) == 1) {
+            // (4) the finish counts for the root; the id goes back unless the
+            //     parent still reads this task's frame
+            bt_release_id(A, S, t, S.flags);
+            bt_credit(A, S, root);
+            // (5) join: the last child resumes its parent on this block, or,
+            //     when the parent's code after its taskwait only finishes,
+            //     books that finish here and goes on to the grandparent
+            int parent = S.parent;
+            bool first = true;
+            while (parent >= 0) {
+                // past the first level this block publishes what it observed
+                // through the previous join (the siblings' data) onwards
+                const int old = first ? atom_add_acquire(&hdr_of(A, parent)->join, -1)
+                                      : atom_add_acq_rel(&hdr_of(A, parent)->join, -1);
+                first = false;
+                if ((old & kJoinCountMask) != 1) break;
+                const int4 ph = ld_cg_v4(hdr_of(A, parent));
+                const unsigned pflags = (unsigned)ph.x >> 24;
+                if (!(pflags & kFlagJoinFinish)) {
                     if (next >= 0) {
                         // the kept child is published after all
-                        fence_acq_rel();
                         ring_push_one(A.overflow, next);
                         S.st[GTAP_STAT_OVERFLOW_PUSHES] += 1;
                     }
                     next = parent;
+                    break;
                 }
+                bt_release_id(A, S, parent, pflags);
+                bt_credit(A, S, ph.w);
+#ifndef GTAP_PHASE_TIMERS
+                S.st[GTAP_STAT_JOIN_FINISHES] += 1;
+#endif
+                parent = ph.y;
             }
-            // (5) the finish counts for the root; the id goes back unless the
-            //     parent still reads this task's frame
-            if (!(S.flags & kFlagRetain)) {
-                if (S.avail_n < kBAvail && S.avail_n >= 0) {
-                    S.avail[S.avail_n++] = t;
-                } else {
-                    ring_push_one(A.idpool, t);
-                }
-            }
-            bt_credit(A, S, root);
         }
         bt_bal_age(A, S);
         S.next = next;
+        S.pre_task = (next >= 0 && next == kept) ? kept : -1;
         S.st[GTAP_STAT_EXECUTIONS] += 1;
         S.st[GTAP_STAT_ROUNDS] += 1;
+    }
+    __syncwarp();
+    // the prefetched record becomes the next task's (orphan marking above
+    // cleared its parent when this task returned without a taskwait)
+    if (kept >= 0 && S.pre_task == kept && lane >= 1 && lane <= 3) {
+        if (lane == 1) {
+            const unsigned x = (unsigned)pre.x;
+            S.state = (int)(x & 0xFFFFu);
+            S.kind = (int)((x >> 16) & 0xFFu);
+            S.flags = (int)(x >> 24);
+            S.parent = (finished && S.spawned > 0) ? -1 : pre.y;
+            S.root = pre.w;
+        } else if (lane == 2) {
+            S.w0 = pre;
+        } else {
+            S.w1 = pre;
+        }
     }
     __syncwarp();
     bt_refill_ids(A, S);
@@ -505,6 +551,24 @@ static __device__ void bt_round_end(const Arena& A, BlockShared& S) {
 // ---------------------------------------------------------------------------
 // the persistent loop
 // ---------------------------------------------------------------------------
+// Profiling builds (-DGTAP_PHASE_TIMERS): thread 0 adds the clock64 cycles of
+// each phase to statistics slots 10..15 (acquire, record load, body, pending
+// children + barrier, round end, idle polls).
+#ifdef GTAP_PHASE_TIMERS
+#define GTAP_BPHASE(t) const long long t = clock64()
+#define GTAP_BPHASE_ADD(slot, a, b) \
+    do {                            \
+        if (tid == 0) S.st[slot] += (unsigned long long)((b) - (a)); \
+    } while (0)
+#else
+#define GTAP_BPHASE(t) \
+    do {               \
+    } while (0)
+#define GTAP_BPHASE_ADD(slot, a, b) \
+    do {                            \
+    } while (0)
+#endif
+
 template <class Prog>
 __device__ void block_worker(const Arena& A, BlockShared& S, int* smem) {
     const int tid = threadIdx.x;
@@ -513,6 +577,7 @@ __device__ void block_worker(const Arena& A, BlockShared& S, int* smem) {
     if (tid == 0) {
         S.worker = blockIdx.x;
         S.next = -1;
+        S.pre_task = -1;
         S.stop = 0;
         S.task = -1;
         S.bump = A.id_base + blockIdx.x * A.ids_per_worker;
@@ -534,6 +599,7 @@ __device__ void block_worker(const Arena& A, BlockShared& S, int* smem) {
     int round = 0;
     __syncthreads();
     for (;;) {
+        GTAP_BPHASE(ph0);
         // ---- acquire (warp 0) ----
         if (w0) {
             int t = -1;
@@ -597,11 +663,19 @@ __device__ void block_worker(const Arena& A, BlockShared& S, int* smem) {
             }
         }
         __syncthreads();
+        GTAP_BPHASE(ph1);
         if (S.stop) break;
         const int t = S.task;
-        if (t < 0) continue;
-        // ---- record: header + first 32 frame bytes ----
-        if (tid < 3) {
+        if (t < 0) {
+            GTAP_BPHASE_ADD(15, ph0, ph1);
+            continue;
+        }
+        GTAP_BPHASE_ADD(10, ph0, ph1);
+        // ---- record: header + first 32 frame bytes (already loaded by the
+        //      last round end when this is the child it kept: every round end
+        //      sets pre_task, and that child is the next task acquired) ----
+        const bool preloaded = S.pre_task == t;
+        if (!preloaded && tid < 3) {
             const int4 v = ld_data_v4(A.records + (size_t)t * A.rec_stride + 16 * tid);
             if (tid == 0) {
                 const unsigned x = (unsigned)v.x;
@@ -617,8 +691,12 @@ __device__ void block_worker(const Arena& A, BlockShared& S, int* smem) {
             }
         }
         __syncthreads();
+        GTAP_BPHASE(ph2);
+        GTAP_BPHASE_ADD(11, ph1, ph2);
         // ---- body (all threads) ----
         Prog::exec(A, S, t, smem);
+        GTAP_BPHASE(ph3);
+        GTAP_BPHASE_ADD(12, ph2, ph3);
         // detached children past the staging list: their frames are written
         // by the threads that spawned them, which publish them
         {
@@ -629,8 +707,12 @@ __device__ void block_worker(const Arena& A, BlockShared& S, int* smem) {
             }
         }
         __syncthreads();
+        GTAP_BPHASE(ph4);
+        GTAP_BPHASE_ADD(13, ph3, ph4);
         if (w0) bt_round_end<Prog>(A, S);
         __syncthreads();
+        GTAP_BPHASE(ph5);
+        GTAP_BPHASE_ADD(14, ph4, ph5);
     }
     __syncthreads();
     if (tid == 0) bt_bal_flush_all(A, S);

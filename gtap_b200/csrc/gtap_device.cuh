@@ -250,6 +250,7 @@ struct TaskHeader {
 static_assert(sizeof(TaskHeader) == kHdrBytes, "header must be 16 bytes");
 
 constexpr uint8_t kFlagRetain = 0x8;
+constexpr uint8_t kFlagJoinFinish = 0x10;   // block mode: after its taskwait the task only finishes
 constexpr uint8_t kKindIndirect = 255;
 constexpr int kJoinCountMask = 0x00FFFFFF;
 

@@ -136,6 +136,7 @@ enum {
     GTAP_STAT_PUBLISHED,          /* tasks made visible to thieves */
     GTAP_STAT_IDLE_POLLS,         /* idle-loop iterations */
     GTAP_STAT_OVERFLOW_PUSHES,
+    GTAP_STAT_JOIN_FINISHES,      /* block mode: continuations that only finish, booked at their join without running */
     GTAP_STAT_COUNT = 16
 };
 
