@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-per-root", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--block-keys", type=int, default=1 << 26,
+                    help="keys of the block-mode cilksort run (cutoffs 2048/2048); 0 = no block run")
     ap.add_argument("--serve-roots", type=int, default=200,
                     help="roots per serve session (BFS on R-MAT 16-20 / tree sums 2^18-2^20); 0 = no serve run")
     ap.add_argument("--config", default="", help="json dict of gtap_config overrides (applied last)")
@@ -350,6 +352,14 @@ def main():
                  "sessions": [{k: r[k] for k in keys} for r in [sv["capacity"]] + sv["sessions"]],
                  "ok": sv["capacity"]["ok"] and all(r["ok"] for r in sv["sessions"])}
 
+    # block-cooperative mode: cilksort of mt19937(42) keys, cutoffs 2048/2048
+    block = None
+    if args.block_keys > 0:
+        gt.gtap_finalize()
+        block = measure_block_cilksort(gt, args.block_keys, args.steps, args.warmup,
+                                       cpu=not args.no_cpu and rank == 0 and world == 1, hbm_peak=hbm,
+                                       overrides=json.loads(args.config) if args.config else {})
+
     cpu = None
     if not args.no_cpu and rank == 0 and world == 1:
         tasks_gpu = [r.tasks for r in res]
@@ -366,7 +376,7 @@ def main():
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "runtime": {k: v for k, v in cfg.as_dict().items()}, "tuned_from": tuned_from},
             "verified": verified, "gpu_launches": 2 * args.steps, "e2e": e2e, "roofline": roof,
-            "cpu_baseline": cpu, "per_root_launch": per_root, "serve": serve, "clocks": ck,
+            "cpu_baseline": cpu, "per_root_launch": per_root, "serve": serve, "block_mode": block, "clocks": ck,
             "scheduler": {"steal_success_rate": counters.get("steal_successes", 0) /
                           max(1, counters.get("steal_attempts", 0)),
                           "idle_polls": counters.get("idle_polls", 0),
@@ -377,6 +387,65 @@ def main():
     gt.gtap_finalize()
     if world > 1:
         dist.destroy_process_group()
+
+
+def cilksort_bytes(n, sort_cutoff):
+    """Algorithmic HBM bytes of cilksort(n): a leaf reads its keys and writes
+    them sorted (8 B/key); an inner node's three merges read and write every
+    key twice (16 B/key) on top of its four quarters."""
+    if n < sort_cutoff:
+        return 8 * n
+    h = n // 2
+    q1, q3 = h // 2, (n - h) // 2
+    return 16 * n + sum(cilksort_bytes(m, sort_cutoff) for m in (q1, h - q1, q3, n - h - q3))
+
+
+def measure_block_cilksort(gt, n, steps, warmup, cpu, hbm_peak, overrides=None):
+    """cilksort of n keys (std::mt19937(42), full int32 range) in block mode,
+    one root per launch, inputs resident; leaves read the pristine input so
+    no restore is needed between launches.  Checked against a plain sort."""
+    import torch
+    keys = gt.gen_keys(42, n)
+    src = torch.from_numpy(keys).cuda()
+    arr = torch.empty_like(src)
+    tmp = torch.empty_like(src)
+    # library defaults (the tuned file is for thread mode) plus explicit overrides
+    gt.gtap_initialize(gt.default_config(**dict(overrides or {}, mode=gt.MODE_BLOCK)))
+    root = gt.cilksort_root(src.data_ptr(), arr.data_ptr(), tmp.data_ptr(), n, 2048, 2048)
+    for _ in range(max(1, warmup)):
+        res, st = gt.launch([root])
+    want = np.sort(keys)
+    ok = bool(np.array_equal(arr.cpu().numpy(), want)) and st.status == 0
+    ms = []
+    for _ in range(steps):
+        res, st = gt.launch([root])
+        ms.append(st.kernel_ms)
+    k_ms = statistics.mean(ms)
+    tasks = res[0].tasks
+    alg = cilksort_bytes(n, 2048)
+    achieved = alg / (k_ms / 1e3) / 1e9
+    out = {"workload": "cilksort of %d int32 keys (std::mt19937(42)), block-cooperative mode, sort and merge "
+                       "cutoffs 2048, one root per launch" % n,
+           "keys": n, "ms_per_sort": k_ms, "keys_per_s": n / (k_ms / 1e3), "tasks": tasks,
+           "tasks_per_s": tasks / (k_ms / 1e3), "grid": st.grid, "block": st.block,
+           "executions": int(st.counters[1]), "join_finishes": int(st.counters[10]),
+           "steal_success_rate": int(st.counters[4]) / max(1, int(st.counters[3])),
+           "sorted_equals_plain_sort": ok,
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                        "frac": achieved / hbm_peak, "algorithmic_bytes_per_launch": alg,
+                        "kernel": "gtap::block_worker_kernel<BlockProgram>"}}
+    gt.gtap_finalize()
+    if cpu:
+        sys.path.insert(0, ROOT)
+        from tests import oracle_lib as orc   # the CPU leg: std::sort of the same keys, one core
+        k2 = keys.copy()
+        t0 = time.perf_counter()
+        orc.load().orc_sort_i32(orc.p(k2), len(k2))
+        wall = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": n / wall, "unit": "keys/s", "cores": 1, "kind": "port",
+                               "sample": "std::sort of the same %d keys (oracle, -O2), %.2f s" % (n, wall),
+                               "matches": bool(np.array_equal(k2, want))}
+    return out
 
 
 def verify(gt, mix, res, src, arr):

@@ -92,7 +92,7 @@ def _signature(gt, res):
     return out
 
 
-def run(workload="mix", reps=3, sweeps=2, n_roots=None, out=None, quiet=False):
+def run(workload="mix", reps=3, sweeps=2, n_roots=None, out=None, quiet=False, start_point=None):
     import torch
     import gtap_b200 as gt
     from gtap_b200 import workloads as wl
@@ -142,6 +142,7 @@ def run(workload="mix", reps=3, sweeps=2, n_roots=None, out=None, quiet=False):
     start = {"warps_per_sm": 8, "block": defaults.block, "deque_capacity": defaults.deque_capacity,
              "steal_batch": defaults.steal_batch, "probe_width": defaults.probe_width,
              "victim_policy": defaults.victim_policy, "num_queues": defaults.num_queues}
+    start.update(start_point or {})
     t0 = time.time()
     best, best_t, trials = coordinate_descent(measure, start, sweeps=sweeps, log=log)
     result = {"workload": workload, "roots": len(roots), "device": torch.cuda.get_device_name(0),
@@ -173,8 +174,9 @@ def main(argv=None):
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--sweeps", type=int, default=2)
     ap.add_argument("--out", default=None)
+    ap.add_argument("--start", default="", help="json point to start the descent from (keys of the search space)")
     a = ap.parse_args(argv)
-    r = run(a.workload, a.reps, a.sweeps, a.roots, a.out)
+    r = run(a.workload, a.reps, a.sweeps, a.roots, a.out, start_point=json.loads(a.start) if a.start else None)
     print(json.dumps({k: r[k] for k in ("workload", "best_point", "best_overrides", "best_kernel_ms", "trials")}))
 
 

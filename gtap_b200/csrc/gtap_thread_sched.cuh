@@ -1183,12 +1183,23 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
                 rt_release_id(A, S, my_tid);
             }
         }
-        // (5) resumed parents take the free lanes of the next batch when they
-        //     belong to its queue; the others go on top of their queue's stack
+        // (5) resumed parents run in the next batch when they belong to its
+        //     queue, before its children: when the batch has no room, its
+        //     oldest children go back on top of their stack (still in place
+        //     above ls_hi), so a continuation is never buried under the next
+        //     round's children.  Parents of other queues, and any beyond 32,
+        //     go on top of their queue's stack.
         const unsigned rmask = __ballot_sync(0xffffffffu, resumed >= 0);
         if (rmask) {
             if (nb_next == 0) kn = __shfl_sync(0xffffffffu, rq, __ffs(rmask) - 1);
             const unsigned inb = __ballot_sync(0xffffffffu, resumed >= 0 && rq == kn);
+            const int d = min(nb_next, max(0, __popc(inb) - (32 - nb_next)));
+            if (d > 0) {
+                qset(P.ls_hi, kn, qget(P.ls_hi, kn) + (unsigned)d);
+                const int v = __shfl_sync(0xffffffffu, next_tid, min((int)lane + d, 31));
+                nb_next -= d;
+                next_tid = (int)lane < nb_next ? v : -1;
+            }
             const int room = 32 - nb_next;
             const int nin = min(__popc(inb), room);
             if ((int)lane >= nb_next && (int)lane < nb_next + nin) {
