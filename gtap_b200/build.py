@@ -29,9 +29,9 @@ LOWERED = os.path.join(ROOT, "tests", "lowered")
 LOWERED_BIN = os.path.join(LOWERED, "bin")
 
 # Programs lowered to the reference's task ABI, built against the drop-in
-# header include/gtap_thread.cuh: (source, binary, -D settings).  "ref"
-# builds use the reference's own evaluation settings, "b200" builds a
-# geometry for 148 SMs.
+# headers include/gtap_thread.cuh and (block mode) include/gtap_block.cuh:
+# (source, binary, -D settings).  "ref" builds use the reference's own
+# evaluation settings, "b200" builds a geometry for 148 SMs.
 LOWERED_BUILDS = [
     ("fib_lowered.cu", "fib_ref_geometry",
      "-DGTAP_GRID_SIZE=4000 -DGTAP_BLOCK_SIZE=32 -DGTAP_MAX_CHILD_TASKS=2"),
@@ -45,6 +45,12 @@ LOWERED_BUILDS = [
      "-DGTAP_GRID_SIZE=2000 -DGTAP_BLOCK_SIZE=32 -DGTAP_MAX_CHILD_TASKS=7"),
     ("cilksort_lowered.cu", "cilksort_b200",
      "-DGTAP_GRID_SIZE=592 -DGTAP_BLOCK_SIZE=128 -DGTAP_MAX_CHILD_TASKS=7"),
+    ("bfs_block_lowered.cu", "bfs_block_ref_geometry",
+     "-DGTAP_GRID_SIZE=4000 -DGTAP_BLOCK_SIZE=32 -DGTAP_MAX_TASKS_PER_BLOCK=150000 -DGTAP_ASSUME_NO_TASKWAIT"),
+    ("bfs_block_lowered.cu", "bfs_block_b200",
+     "-DGTAP_GRID_SIZE=1184 -DGTAP_BLOCK_SIZE=256 -DGTAP_MAX_TASKS_PER_BLOCK=20000 -DGTAP_ASSUME_NO_TASKWAIT"),
+    ("tree_block_lowered.cu", "tree_block_ref_geometry", "-DGTAP_GRID_SIZE=4000 -DGTAP_BLOCK_SIZE=32"),
+    ("tree_block_lowered.cu", "tree_block_b200", "-DGTAP_GRID_SIZE=1184 -DGTAP_BLOCK_SIZE=128"),
 ]
 
 

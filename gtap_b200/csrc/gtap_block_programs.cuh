@@ -379,6 +379,7 @@ __device__ void treesum_task(const Arena& A, BlockShared& S) {
 // leaf sizes bounded by what one block stages in shared memory.
 struct BlockProgram {
     static constexpr int kSmemInts = bprog::kSmemInts;
+    static constexpr bool kFuncTable = false;
     __device__ static int root_kind(int k) { return BuiltinProgram::root_kind(k); }
     __device__ static bool root_args_ok(const gtap_root& rd) {
         if (!BuiltinProgram::root_args_ok(rd)) return false;

@@ -33,12 +33,14 @@ constexpr int kBAvail = 256;         // free ids cached per block
 constexpr int kBAvailLow = 96;       // refill below this many
 constexpr int kBMaxThreads = 512;    // threads per block in block mode (a leaf task's width)
 constexpr int kBBal = 4;             // roots with a pre-charged balance per block
+constexpr int kBRel = 64;            // ids released by task code in one execution, returned at round end
 constexpr int kBChunk = 256;         // credit taken from a root's counter at a time
 
 struct BlockShared {
     // the task this execution runs (written by warp 0 before the body)
     int task, kind, state, flags, parent, root;
     int4 w0, w1;                     // the frame's first 32 bytes
+    unsigned long long fn;           // task function (programs with a function table)
     // spawn bookkeeping of this execution
     int nstaged;                     // children staged (beyond kBStage: waited per thread)
     int spawned;                     // children that join this task, since its last taskwait
@@ -56,6 +58,8 @@ struct BlockShared {
     int avail[kBAvail];
     int staged[kBStage];
     int pend[kBMaxThreads];          // per thread: a detached child past kBStage whose frame is being written
+    int nrel;                        // ids task code released this execution (bt_release_deferred)
+    int rel[kBRel];
     unsigned long long st[GTAP_STAT_COUNT];
     // pre-charged balances: the block holds credit[i] units of root bal_root[i]'s
     // outstanding count; finishes add to it, creations draw on it
@@ -191,6 +195,21 @@ __device__ __forceinline__ void bt_return_i32(const Arena& A, const BlockShared&
 // Any thread: add to the root's value (n-queens counts).
 __device__ __forceinline__ void bt_add_value(BlockShared& S, long long v) {
     atomicAdd(reinterpret_cast<unsigned long long*>(&S.value), (unsigned long long)v);
+}
+
+// Any thread: a retained child's id, once its frame has been read.  It goes
+// back at round end, after the barrier that ends the body, so no thread of
+// the block can still be reading the frame; past kBRel per execution it goes
+// to the recycled-id ring at once (the caller has finished reading it).
+__device__ __forceinline__ void bt_release_deferred(const Arena& A, BlockShared& S, int id) {
+    if ((unsigned)id >= (unsigned)A.total_ids) return;
+    const int k = atomicAdd(&S.nrel, 1);
+    if (k < kBRel) {
+        S.rel[k] = id;
+    } else {
+        fence_acq_rel();
+        ring_push_one(A.idpool, id);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -433,7 +452,9 @@ static __device__ void bt_round_end(const Arena& A, BlockShared& S) {
     // it, before the barrier that precedes round end)
     const int kept = n_st > 0 ? S.staged[n_st - 1] : -1;
     int4 pre = make_int4(0, 0, 0, 0);
+    unsigned long long pre_fn = 0;
     if (kept >= 0 && lane >= 1 && lane <= 3) pre = ld_data_v4(A.records + (size_t)kept * A.rec_stride + 16 * (lane - 1));
+    if (Prog::kFuncTable && kept >= 0 && lane == 4) pre_fn = ld_data_u64(reinterpret_cast<const unsigned long long*>(A.funcs + kept));
     // (1) the round's value and its children count for the root before any
     //     child can be seen by another block
     if (lane == 0) {
@@ -485,6 +506,8 @@ static __device__ void bt_round_end(const Arena& A, BlockShared& S) {
             S.st[GTAP_STAT_PUBLISHED] += (unsigned long long)direct;
         }
         int next = kept;
+        // ids the task code released (retained children it has read)
+        for (int i = 0; i < min(S.nrel, kBRel); ++i) bt_release_id(A, S, S.rel[i], 0);
         if (finished) {
             // (4) the finish counts for the root; the id goes back unless the
             //     parent still reads this task's frame
@@ -530,6 +553,7 @@ static __device__ void bt_round_end(const Arena& A, BlockShared& S) {
     __syncwarp();
     // the prefetched record becomes the next task's (orphan marking above
     // cleared its parent when this task returned without a taskwait)
+    if (Prog::kFuncTable && kept >= 0 && S.pre_task == kept && lane == 4) S.fn = pre_fn;
     if (kept >= 0 && S.pre_task == kept && lane >= 1 && lane <= 3) {
         if (lane == 1) {
             const unsigned x = (unsigned)pre.x;
@@ -569,14 +593,16 @@ static __device__ void bt_round_end(const Arena& A, BlockShared& S) {
     } while (0)
 #endif
 
+// initial_tid >= 0: this block starts with that task (one created before the
+// loop, e.g. by the drop-in __gtap_push_initial_task).
 template <class Prog>
-__device__ void block_worker(const Arena& A, BlockShared& S, int* smem) {
+__device__ void block_worker(const Arena& A, BlockShared& S, int* smem, int initial_tid = -1) {
     const int tid = threadIdx.x;
     const unsigned lane = lane_id();
     const bool w0 = tid < 32;
     if (tid == 0) {
         S.worker = blockIdx.x;
-        S.next = -1;
+        S.next = initial_tid;
         S.pre_task = -1;
         S.stop = 0;
         S.task = -1;
@@ -655,6 +681,7 @@ __device__ void block_worker(const Arena& A, BlockShared& S, int* smem) {
                 }
                 S.stop = stop;
                 S.task = t;
+                S.nrel = 0;
                 S.nstaged = 0;
                 S.spawned = 0;
                 S.suspended = 0;
@@ -675,6 +702,7 @@ __device__ void block_worker(const Arena& A, BlockShared& S, int* smem) {
         //      last round end when this is the child it kept: every round end
         //      sets pre_task, and that child is the next task acquired) ----
         const bool preloaded = S.pre_task == t;
+        if (Prog::kFuncTable && !preloaded && tid == 3) S.fn = ld_data_u64(reinterpret_cast<const unsigned long long*>(A.funcs + t));
         if (!preloaded && tid < 3) {
             const int4 v = ld_data_v4(A.records + (size_t)t * A.rec_stride + 16 * tid);
             if (tid == 0) {
