@@ -433,6 +433,8 @@ def measure_block_cilksort(gt, n, steps, warmup, cpu, hbm_peak, overrides=None):
            "sorted_equals_plain_sort": ok,
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                         "frac": achieved / hbm_peak, "algorithmic_bytes_per_launch": alg,
+                        "traffic": (None if traffic_from_profile("block_kernel_traffic_over_algorithmic") is None
+                                    else int(alg * traffic_from_profile("block_kernel_traffic_over_algorithmic"))),
                         "kernel": "gtap::block_worker_kernel<BlockProgram>"}}
     gt.gtap_finalize()
     if cpu:
@@ -511,11 +513,11 @@ def measure_e2e(gt, mix, steps, tasks_per_step, world, arr_dev):
             "ok": ok}
 
 
-def traffic_from_profile():
-    """DRAM bytes per launch of the worker kernel from the committed ncu summary, if any."""
+def traffic_from_profile(key="worker_kernel_dram_bytes_per_launch"):
+    """A figure from the committed ncu summary of DRAM traffic, if any."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     try:
-        return json.load(open(p)).get("worker_kernel_dram_bytes_per_launch")
+        return json.load(open(p)).get(key)
     except Exception:
         return None
 
