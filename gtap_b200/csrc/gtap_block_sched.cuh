@@ -51,6 +51,8 @@ struct BlockShared {
     int pre_task;                    // the task whose record round end already loaded into the fields above
     int stop;
     int worker;
+    int prof_h, prof_w;              // samples written to this block's profile timelines
+    int having;                      // profile: the block holds a task (since its last idle poll)
     // id cache
     int avail_n;
     int bump;                        // next id of the private range
@@ -264,6 +266,27 @@ static __device__ void bt_bal_age(const Arena& A, BlockShared& S) {
 }
 static __device__ void bt_bal_flush_all(const Arena& A, BlockShared& S) {
     while (S.nbal > 0) bt_bal_flush(A, S, S.nbal - 1);
+}
+
+// ---------------------------------------------------------------------------
+// profile timelines (reference runtime/detail/block/gtap_profile_block.cuh):
+// one row per block; "having task" spans open when the block finds work after
+// an idle poll and close at the next idle poll, "working" spans cover each
+// task execution (thread 0 writes both)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void bt_prof_having(const Arena& A, BlockShared& S) {
+    if (A.prof_cap > 0 && S.prof_h < A.prof_cap) {
+        A.prof_having[(size_t)S.worker * A.prof_cap + S.prof_h] = (long long)global_ns();
+        S.prof_h++;
+    }
+}
+__device__ __forceinline__ void bt_prof_working(const Arena& A, BlockShared& S) {
+    if (A.prof_cap > 0 && S.prof_w < A.prof_cap) {
+        const size_t i = (size_t)S.worker * A.prof_cap + S.prof_w;
+        A.prof_working[i] = (long long)global_ns();
+        A.prof_tasks[i] = 1;
+        S.prof_w++;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -610,6 +633,9 @@ __device__ void block_worker(const Arena& A, BlockShared& S, int* smem, int init
         S.bump_end = S.bump + A.ids_per_worker;
         S.avail_n = 0;
         S.nbal = 0;
+        S.prof_h = 0;
+        S.prof_w = 0;
+        S.having = 0;
         for (int i = 0; i < GTAP_STAT_COUNT; ++i) S.st[i] = 0;
     }
     for (int i = tid; i < kBMaxThreads; i += blockDim.x) S.pend[i] = -1;
@@ -648,6 +674,10 @@ __device__ void block_worker(const Arena& A, BlockShared& S, int* smem, int init
                 if (t < 0) {
                     S.st[GTAP_STAT_IDLE_POLLS] += 1;
                     bt_bal_flush_all(A, S);
+                    if (S.having) {
+                        bt_prof_having(A, S);
+                        S.having = 0;
+                    }
                     if (ld_acquire(A.done_flag) != 0 || aborted(A)) stop = 1;
                     if (A.mode == 2 && ld_relaxed(A.shutdown) != 0) {
                         const unsigned pub = ld_acquire(A.published);
@@ -671,6 +701,10 @@ __device__ void block_worker(const Arena& A, BlockShared& S, int* smem, int init
                     __nanosleep(32u << backoff);
                 } else {
                     backoff = 0;
+                    if (!S.having) {
+                        bt_prof_having(A, S);
+                        S.having = 1;
+                    }
                     if ((++round & 63) == 0) {
                         if (aborted(A)) stop = 1;
                         else if (A.mode != 2 && global_ns() - t_watch > A.watchdog_ns) {
@@ -722,6 +756,7 @@ __device__ void block_worker(const Arena& A, BlockShared& S, int* smem, int init
         GTAP_BPHASE(ph2);
         GTAP_BPHASE_ADD(11, ph1, ph2);
         // ---- body (all threads) ----
+        if (tid == 0) bt_prof_working(A, S);
         Prog::exec(A, S, t, smem);
         GTAP_BPHASE(ph3);
         GTAP_BPHASE_ADD(12, ph2, ph3);
@@ -738,6 +773,7 @@ __device__ void block_worker(const Arena& A, BlockShared& S, int* smem, int init
         GTAP_BPHASE(ph4);
         GTAP_BPHASE_ADD(13, ph3, ph4);
         if (w0) bt_round_end<Prog>(A, S);
+        if (tid == 0) bt_prof_working(A, S);
         __syncthreads();
         GTAP_BPHASE(ph5);
         GTAP_BPHASE_ADD(14, ph4, ph5);

@@ -1003,7 +1003,8 @@ void ensure_dir(const char* path) {
 
 extern "C" int gtap_write_profile(const char* directory, const char* app_name) {
     if (!g.initialized || !g.have_profile || !directory || !app_name) return GTAP_ERROR_INVALID_ARGUMENT;
-    const int W = g.workers, P = g.cfg.profile_samples;
+    // one row per worker of the last launch (warps, or blocks in block mode)
+    const int W = g.last_workers > 0 ? std::min(g.last_workers, g.workers) : g.workers, P = g.cfg.profile_samples;
     std::vector<long long> hv((size_t)W * P), wv((size_t)W * P);
     std::vector<int> tv((size_t)W * P);
     GT_CUDA(cudaMemcpy(hv.data(), g.prof_having, hv.size() * sizeof(long long), cudaMemcpyDeviceToHost));
