@@ -288,11 +288,7 @@ def main():
     if world > 1:
         dist.barrier()
     ck = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(e0.elapsed_time(e1), world, "cuda")
     tasks_per_step = int(statistics.median(tasks_step))
     value = world * tasks_per_step * args.steps / (ms_max / 1e3)
 
@@ -387,6 +383,16 @@ def main():
     gt.gtap_finalize()
     if world > 1:
         dist.destroy_process_group()
+
+
+def max_over_ranks(x, world, device):
+    """The largest of every rank's x (the job's time is its slowest rank's)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def cilksort_bytes(n, sort_cutoff):
