@@ -1078,12 +1078,44 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
             }
             __syncwarp();
         }
-        // (2) this round's children join their queue's local stack (newest on
-        //     top); the busiest queue's newest <= 32 run next (reference
+        // (2) one warp-wide fence orders this round's stores (children's
+        //     records, results written into parents' frames, orphan marks)
+        //     before the join decrements, which therefore need only acquire
+        //     semantics.
+        const unsigned joiners = __ballot_sync(0xffffffffu, my_fin && S.l_parent[lane] >= 0);
+        if (joiners) {
+            fence_acq_rel();
+            __syncwarp();
+        }
+        GTAP_PHASE_MARK(ph3);
+        GTAP_PHASE_ADD(12, ph2, ph3);
+        // (3) joins: the last child re-enqueues its parent on the resume queue;
+        //     release the finished task's id unless its parent reads its frame
+        int resumed = -1, rq = 0;
+        if (my_fin) {
+            const int parent = S.l_parent[lane];
+            if (parent >= 0) {
+                const int old = atom_add_acquire(&hdr_of(A, parent)->join, -1);
+                if ((old & kJoinCountMask) == 1) {
+                    rq = (old >> 24) & 7;
+                    if (rq >= A.num_queues) rq = 0;
+                    resumed = parent;
+                }
+            }
+            if (!(lane_flags & kLaneRetain)) {
+                rt_release_id_dbg(A, my_tid);
+                rt_release_id(A, S, my_tid);
+            }
+        }
+        const unsigned rmask = __ballot_sync(0xffffffffu, resumed >= 0);
+        GTAP_PHASE_MARK(ph3b);
+        GTAP_PHASE_ADD(7, ph3, ph3b);
+        // (4) this round's children join their queue's local stack, and the
+        //     parents they resumed go on top of them (newest), so continuations
+        //     run first; the busiest queue's newest <= 32 run next (reference
         //     push_batch keeps the newest 32 of k_max); the oldest entries are
         //     written to the deque when a stack overflows or some worker is
-        //     hungry (always, with eager publication).  Slot stores only: the
-        //     fence in (3) publishes them.
+        //     hungry (always, with eager publication), and published in (5).
         int kn = -1;
         {
             const int Q = A.num_queues;
@@ -1091,30 +1123,38 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
             const int hungry = A.publish_lazy ? __shfl_sync(0xffffffffu, hv, 0) : 1;
             const int reserve = A.publish_lazy ? kReserve : 0;
             int best = 0;
-            for (int k = 0; k < Q; ++k)
-                if (S.cnt[k] > best) {
-                    best = S.cnt[k];
+            for (int k = 0; k < Q; ++k) {
+                const int c = S.cnt[k] + (rmask ? __popc(__ballot_sync(0xffffffffu, resumed >= 0 && rq == k)) : 0);
+                if (c > best) {
+                    best = c;
                     kn = k;
                 }
+            }
             for (int k = 0; k < Q; ++k) {
                 const int n = min(S.cnt[k], A.spawn_cap);
-                if (n == 0) continue;
+                const unsigned mk = rmask ? __ballot_sync(0xffffffffu, resumed >= 0 && rq == k) : 0u;
+                const int add = __popc(mk);
+                if (n == 0 && add == 0) continue;
                 const int* sb = S.sbuf + k * A.spawn_cap;
                 int* ls = S.lstk + k * kLocalCap;
                 const unsigned lo = qget(P.ls_lo, k), hi = qget(P.ls_hi, k);
                 const int size = (int)(hi - lo);
-                const int over = size + n - kLocalCap;
+                // kLocalCap (128) >= 32 resumed parents: the overflow comes
+                // from the stack and the children only
+                const int over = size + n + add - kLocalCap;
                 int from_sb = 0;
                 if (over > 0) {
                     const int m1 = min(over, size);
                     if (m1 > 0) publish_stage(A, S, P, k, ls, lo, kLocalCap - 1, m1);
-                    from_sb = over - m1;
+                    from_sb = min(over - m1, n);
                     if (from_sb > 0) publish_stage(A, S, P, k, sb, 0, 0xFFFFFFFFu, from_sb);
                     qset(P.ls_lo, k, lo + (unsigned)m1);
                 }
                 for (int e = from_sb + (int)lane; e < n; e += 32)
                     ls[(hi + (unsigned)(e - from_sb)) & (kLocalCap - 1)] = sb[e] & kIdMask;
-                qset(P.ls_hi, k, hi + (unsigned)(n - from_sb));
+                const unsigned h2 = hi + (unsigned)(n - from_sb);
+                if ((mk >> lane) & 1u) ls[(h2 + (unsigned)__popc(mk & ((1u << lane) - 1u))) & (kLocalCap - 1)] = resumed;
+                qset(P.ls_hi, k, h2 + (unsigned)add);
             }
             __syncwarp();   // local-stack entries written above are read below by other lanes
             if (kn < 0) {
@@ -1142,6 +1182,7 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
                 qset(P.ls_hi, kn, hi - (unsigned)take);
                 P.cur_q = kn;
             }
+            __syncwarp();   // batch entries were read from the local stacks before they are published
             if (hungry > 0) {
                 // keep one more batch in reserve so the next rounds stay full
                 for (int k = 0; k < Q; ++k) {
@@ -1155,82 +1196,9 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
                 }
             }
         }
-        GTAP_PHASE_MARK(ph3);
-        GTAP_PHASE_ADD(12, ph2, ph3);
-        // (3) one warp-wide fence orders this round's stores (children's
-        //     records, results written into parents' frames, orphan marks,
-        //     deque slots) before the publication and before the join
-        //     decrements, which therefore need only acquire semantics.
-        const unsigned joiners = __ballot_sync(0xffffffffu, my_fin && S.l_parent[lane] >= 0);
-        publish_commit(A, S, P, joiners != 0);
-        GTAP_PHASE_MARK(ph3b);
-        GTAP_PHASE_ADD(7, ph3, ph3b);
-        // (4) joins: the last child re-enqueues its parent on the resume queue;
-        //     release the finished task's id unless its parent reads its frame
-        int resumed = -1, rq = 0;
-        if (my_fin) {
-            const int parent = S.l_parent[lane];
-            if (parent >= 0) {
-                const int old = atom_add_acquire(&hdr_of(A, parent)->join, -1);
-                if ((old & kJoinCountMask) == 1) {
-                    rq = (old >> 24) & 7;
-                    if (rq >= A.num_queues) rq = 0;
-                    resumed = parent;
-                }
-            }
-            if (!(lane_flags & kLaneRetain)) {
-                rt_release_id_dbg(A, my_tid);
-                rt_release_id(A, S, my_tid);
-            }
-        }
-        // (5) resumed parents run in the next batch when they belong to its
-        //     queue, before its children: when the batch has no room, its
-        //     oldest children go back on top of their stack (still in place
-        //     above ls_hi), so a continuation is never buried under the next
-        //     round's children.  Parents of other queues, and any beyond 32,
-        //     go on top of their queue's stack.
-        const unsigned rmask = __ballot_sync(0xffffffffu, resumed >= 0);
-        if (rmask) {
-            if (nb_next == 0) kn = __shfl_sync(0xffffffffu, rq, __ffs(rmask) - 1);
-            const unsigned inb = __ballot_sync(0xffffffffu, resumed >= 0 && rq == kn);
-            const int d = min(nb_next, max(0, __popc(inb) - (32 - nb_next)));
-            if (d > 0) {
-                qset(P.ls_hi, kn, qget(P.ls_hi, kn) + (unsigned)d);
-                const int v = __shfl_sync(0xffffffffu, next_tid, min((int)lane + d, 31));
-                nb_next -= d;
-                next_tid = (int)lane < nb_next ? v : -1;
-            }
-            const int room = 32 - nb_next;
-            const int nin = min(__popc(inb), room);
-            if ((int)lane >= nb_next && (int)lane < nb_next + nin) {
-                const int src = (int)__fns(inb, 0, (int)lane - nb_next + 1);
-                next_tid = -2 - src;   // filled from lane src below
-            }
-            const int v = __shfl_sync(0xffffffffu, resumed, next_tid <= -2 ? -2 - next_tid : 0);
-            if (next_tid <= -2) next_tid = v;
-            // resumed lanes that did not get a slot: all but the first nin of inb
-            const unsigned placed = nin > 0 ? (inb & ((2u << __fns(inb, 0, nin)) - 1u)) : 0u;
-            const unsigned rest = rmask & ~placed;
-            if (nin > 0) P.cur_q = kn;
-            __syncwarp();   // batch entries were read from the local stacks before they are reused
-            nb_next += nin;
-            for (int k = 0; rest && k < A.num_queues; ++k) {
-                const unsigned mk = __ballot_sync(0xffffffffu, ((rest >> lane) & 1u) && rq == k);
-                if (!mk) continue;
-                int* ls = S.lstk + k * kLocalCap;
-                const unsigned lo = qget(P.ls_lo, k), hi = qget(P.ls_hi, k);
-                const int add = __popc(mk);
-                const int over = (int)(hi - lo) + add - kLocalCap;
-                if (over > 0) {   // a full stack: its oldest entries go to the deque first (rare)
-                    publish_stage(A, S, P, k, ls, lo, kLocalCap - 1, over);
-                    publish_commit(A, S, P, false);
-                    qset(P.ls_lo, k, lo + (unsigned)over);
-                }
-                if ((mk >> lane) & 1u) ls[(hi + (unsigned)__popc(mk & ((1u << lane) - 1u))) & (kLocalCap - 1)] = resumed;
-                qset(P.ls_hi, k, hi + (unsigned)add);
-                __syncwarp();
-            }
-        }
+        // (5) publication of the deque entries staged above (its own fence:
+        //     the slot stores, and the records when nothing joined)
+        publish_commit(A, S, P, false);
         GTAP_PHASE_MARK(ph4);
         GTAP_PHASE_ADD(13, ph3b, ph4);
         // (6) per-root accounting of finishes and values (creations were
