@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--block-keys", type=int, default=1 << 26,
                     help="keys of the block-mode cilksort run (cutoffs 2048/2048); 0 = no block run")
+    ap.add_argument("--mergesort-keys", type=int, default=1 << 24,
+                    help="keys of the thread-mode mergesort run (cutoff 128); 0 = no mergesort run")
     ap.add_argument("--serve-roots", type=int, default=200,
                     help="roots per serve session (BFS on R-MAT 16-20 / tree sums 2^18-2^20); 0 = no serve run")
     ap.add_argument("--config", default="", help="json dict of gtap_config overrides (applied last)")
@@ -356,6 +358,13 @@ def main():
                                        cpu=not args.no_cpu and rank == 0 and world == 1, hbm_peak=hbm,
                                        overrides=json.loads(args.config) if args.config else {})
 
+    # thread mode: mergesort of mt19937(42) keys (examples/mergesort/mergesort.cu's cutoff 128)
+    msort = None
+    if args.mergesort_keys > 0:
+        gt.gtap_finalize()
+        msort = measure_mergesort_thread(gt, args.mergesort_keys, args.steps, args.warmup, hbm_peak=hbm,
+                                         overrides=json.loads(args.config) if args.config else {})
+
     cpu = None
     if not args.no_cpu and rank == 0 and world == 1:
         tasks_gpu = [r.tasks for r in res]
@@ -372,7 +381,8 @@ def main():
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "runtime": {k: v for k, v in cfg.as_dict().items()}, "tuned_from": tuned_from},
             "verified": verified, "gpu_launches": 2 * args.steps, "e2e": e2e, "roofline": roof,
-            "cpu_baseline": cpu, "per_root_launch": per_root, "serve": serve, "block_mode": block, "clocks": ck,
+            "cpu_baseline": cpu, "per_root_launch": per_root, "serve": serve, "block_mode": block, "mergesort_thread": msort,
+            "clocks": ck,
             "scheduler": {"steal_success_rate": counters.get("steal_successes", 0) /
                           max(1, counters.get("steal_attempts", 0)),
                           "idle_polls": counters.get("idle_polls", 0),
@@ -404,6 +414,46 @@ def cilksort_bytes(n, sort_cutoff):
     h = n // 2
     q1, q3 = h // 2, (n - h) // 2
     return 16 * n + sum(cilksort_bytes(m, sort_cutoff) for m in (q1, h - q1, q3, n - h - q3))
+
+
+def mergesort_bytes(n, cutoff):
+    """Algorithmic HBM bytes of mergesort(n): a leaf reads its keys and writes
+    them sorted, every merge reads and writes the keys of its node (8 B/key)."""
+    if n <= cutoff or n <= 1:
+        return 8 * n
+    nl = (n + 1) // 2
+    return 8 * n + mergesort_bytes(nl, cutoff) + mergesort_bytes(n - nl, cutoff)
+
+
+def measure_mergesort_thread(gt, n, steps, warmup, hbm_peak, overrides=None):
+    """mergesort of n keys (std::mt19937(42)) in thread mode, cutoff 128 and
+    merge cutoff 256, one root per launch with the library defaults (plus
+    explicit overrides); checked against a plain sort."""
+    import torch
+    keys = gt.gen_keys(42, n)
+    src = torch.from_numpy(keys).cuda()
+    out = torch.empty_like(src)
+    tmp = torch.empty_like(src)
+    gt.gtap_initialize(gt.default_config(**dict(overrides or {})))
+    root = gt.mergesort_root(src.data_ptr(), out.data_ptr(), tmp.data_ptr(), n, 128, 256)
+    for _ in range(max(1, warmup)):
+        res, st = gt.launch([root])
+    ok = bool(np.array_equal(out.cpu().numpy(), np.sort(keys))) and st.status == 0
+    ms = []
+    for _ in range(steps):
+        res, st = gt.launch([root])
+        ms.append(st.kernel_ms)
+    gt.gtap_finalize()
+    k_ms = statistics.mean(ms)
+    alg = mergesort_bytes(n, 128)
+    achieved = alg / (k_ms / 1e3) / 1e9
+    return {"workload": "mergesort of %d int32 keys (std::mt19937(42)), thread mode, cutoff 128, merge cutoff 256, "
+                        "one root per launch" % n,
+            "keys": n, "ms_per_sort": k_ms, "keys_per_s": n / (k_ms / 1e3), "tasks": res[0].tasks,
+            "tasks_per_s": res[0].tasks / (k_ms / 1e3), "sorted_equals_plain_sort": ok,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": achieved / hbm_peak, "algorithmic_bytes_per_launch": alg,
+                         "kernel": "gtap::thread_worker_kernel<BuiltinProgram>"}}
 
 
 def measure_block_cilksort(gt, n, steps, warmup, cpu, hbm_peak, overrides=None):
