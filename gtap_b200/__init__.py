@@ -141,6 +141,11 @@ _SIGS = [
     ("gtap_gen_keys", ctypes.c_int, [ctypes.c_uint32, ctypes.c_void_p, ctypes.c_int64]),
     ("gtap_gen_mix", ctypes.c_int, [ctypes.c_uint64, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("gtap_gen_rmat", ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p]),
+    ("gtap_read_array_file", ctypes.c_int, [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
+    ("gtap_write_array_file", ctypes.c_int, [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int64]),
+    ("gtap_read_csr_file", ctypes.c_int, [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
+                                          ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]),
+    ("gtap_write_csr_file", ctypes.c_int, [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32]),
     ("gtap_gen_tree", ctypes.c_int,
      [ctypes.c_int32, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
 ]
@@ -364,6 +369,40 @@ def gen_tree(n, seed=42):
     size = np.empty(n, np.int32)
     _check(lib().gtap_gen_tree(n, seed, _ptr(left), _ptr(right), _ptr(value), _ptr(size)), "gtap_gen_tree")
     return left, right, value, size
+
+
+# ---- the reference's input files ------------------------------------------------
+def read_array(path):
+    """An int32 array in the reference's gen_vector format (size_t n, int32[n])."""
+    n = ctypes.c_int64(0)
+    _check(lib().gtap_read_array_file(str(path).encode(), None, 0, ctypes.byref(n)), "gtap_read_array_file")
+    out = np.empty(n.value, np.int32)
+    _check(lib().gtap_read_array_file(str(path).encode(), _ptr(out), n.value, ctypes.byref(n)), "gtap_read_array_file")
+    return out
+
+
+def write_array(path, a):
+    a = np.ascontiguousarray(a, dtype=np.int32)
+    _check(lib().gtap_write_array_file(str(path).encode(), _ptr(a), len(a)), "gtap_write_array_file")
+
+
+def read_csr(path):
+    """(row, col) from the reference's CSR binary (int N, int M, row[N+1], col[M])."""
+    n, m = ctypes.c_int32(0), ctypes.c_int32(0)
+    _check(lib().gtap_read_csr_file(str(path).encode(), None, 0, None, 0, ctypes.byref(n), ctypes.byref(m)),
+           "gtap_read_csr_file")
+    row = np.empty(n.value + 1, np.int32)
+    col = np.empty(m.value, np.int32)
+    _check(lib().gtap_read_csr_file(str(path).encode(), _ptr(row), len(row), _ptr(col), len(col), ctypes.byref(n),
+                                    ctypes.byref(m)), "gtap_read_csr_file")
+    return row, col
+
+
+def write_csr(path, row, col):
+    row = np.ascontiguousarray(row, dtype=np.int32)
+    col = np.ascontiguousarray(col, dtype=np.int32)
+    _check(lib().gtap_write_csr_file(str(path).encode(), _ptr(row), _ptr(col), len(row) - 1, len(col)),
+           "gtap_write_csr_file")
 
 
 def max_degree_vertex(row):

@@ -1151,6 +1151,89 @@ extern "C" int gtap_gen_rmat(int32_t scale, int32_t edge_factor, uint64_t seed, 
     return 0;
 }
 
+// ---------------------------------------------------------------------------
+// on-disk formats of the reference's inputs
+// ---------------------------------------------------------------------------
+namespace {
+struct File {
+    FILE* f;
+    explicit File(FILE* p) : f(p) {}
+    ~File() {
+        if (f) fclose(f);
+    }
+};
+long long file_bytes(FILE* f) {
+    if (fseek(f, 0, SEEK_END) != 0) return -1;
+    const long long b = ftell(f);
+    if (fseek(f, 0, SEEK_SET) != 0) return -1;
+    return b;
+}
+}  // namespace
+
+// evaluation/util/gen_vector.c:21-60: size_t n, then n int32 values.
+extern "C" int gtap_read_array_file(const char* path, int32_t* out, int64_t capacity, int64_t* n_out) {
+    if (!path || !n_out || capacity < 0) return GTAP_ERROR_INVALID_ARGUMENT;
+    File fp(fopen(path, "rb"));
+    if (!fp.f) return GTAP_ERROR_INVALID_ARGUMENT;
+    const long long bytes = file_bytes(fp.f);
+    uint64_t n = 0;
+    if (bytes < 8 || fread(&n, sizeof(n), 1, fp.f) != 1) return GTAP_ERROR_INVALID_ARGUMENT;
+    if (n > (uint64_t)INT64_MAX / 4 || (long long)(8 + 4 * n) != bytes) return GTAP_ERROR_INVALID_ARGUMENT;
+    *n_out = (int64_t)n;
+    if (!out) return 0;   // size query
+    if ((uint64_t)capacity < n) return GTAP_ERROR_INVALID_ARGUMENT;
+    if (n && fread(out, sizeof(int32_t), n, fp.f) != n) return GTAP_ERROR_INVALID_ARGUMENT;
+    return 0;
+}
+
+extern "C" int gtap_write_array_file(const char* path, const int32_t* data, int64_t n) {
+    if (!path || n < 0 || (n > 0 && !data)) return GTAP_ERROR_INVALID_ARGUMENT;
+    File fp(fopen(path, "wb"));
+    if (!fp.f) return GTAP_ERROR_INVALID_ARGUMENT;
+    const uint64_t un = (uint64_t)n;
+    if (fwrite(&un, sizeof(un), 1, fp.f) != 1) return GTAP_ERROR_INVALID_ARGUMENT;
+    if (n && fwrite(data, sizeof(int32_t), (size_t)n, fp.f) != (size_t)n) return GTAP_ERROR_INVALID_ARGUMENT;
+    return 0;
+}
+
+// examples/asynchronous_bfs/asynchronous_bfs_thread.cu:69-84: int N, int M,
+// int row[N+1], int col[M].  The offsets must start at 0, never decrease and
+// end at M, and every column must name a vertex.
+extern "C" int gtap_read_csr_file(const char* path, int32_t* row, int64_t row_capacity, int32_t* col,
+                                  int64_t col_capacity, int32_t* n_out, int32_t* m_out) {
+    if (!path || !n_out || !m_out) return GTAP_ERROR_INVALID_ARGUMENT;
+    File fp(fopen(path, "rb"));
+    if (!fp.f) return GTAP_ERROR_INVALID_ARGUMENT;
+    const long long bytes = file_bytes(fp.f);
+    int32_t hdr[2];
+    if (bytes < 8 || fread(hdr, sizeof(int32_t), 2, fp.f) != 2) return GTAP_ERROR_INVALID_ARGUMENT;
+    const int32_t N = hdr[0], M = hdr[1];
+    if (N < 0 || M < 0 || 8 + 4 * ((long long)N + 1 + M) != bytes) return GTAP_ERROR_INVALID_ARGUMENT;
+    *n_out = N;
+    *m_out = M;
+    if (!row && !col) return 0;   // size query
+    if (!row || !col || row_capacity < (int64_t)N + 1 || col_capacity < M) return GTAP_ERROR_INVALID_ARGUMENT;
+    if (fread(row, sizeof(int32_t), (size_t)N + 1, fp.f) != (size_t)N + 1) return GTAP_ERROR_INVALID_ARGUMENT;
+    if (M && fread(col, sizeof(int32_t), (size_t)M, fp.f) != (size_t)M) return GTAP_ERROR_INVALID_ARGUMENT;
+    if (row[0] != 0 || row[N] != M) return GTAP_ERROR_INVALID_ARGUMENT;
+    for (int32_t v = 0; v < N; ++v)
+        if (row[v + 1] < row[v]) return GTAP_ERROR_INVALID_ARGUMENT;
+    for (int32_t e = 0; e < M; ++e)
+        if (col[e] < 0 || col[e] >= N) return GTAP_ERROR_INVALID_ARGUMENT;
+    return 0;
+}
+
+extern "C" int gtap_write_csr_file(const char* path, const int32_t* row, const int32_t* col, int32_t n, int32_t m) {
+    if (!path || n < 0 || m < 0 || !row || (m > 0 && !col)) return GTAP_ERROR_INVALID_ARGUMENT;
+    File fp(fopen(path, "wb"));
+    if (!fp.f) return GTAP_ERROR_INVALID_ARGUMENT;
+    const int32_t hdr[2] = {n, m};
+    if (fwrite(hdr, sizeof(int32_t), 2, fp.f) != 2) return GTAP_ERROR_INVALID_ARGUMENT;
+    if (fwrite(row, sizeof(int32_t), (size_t)n + 1, fp.f) != (size_t)n + 1) return GTAP_ERROR_INVALID_ARGUMENT;
+    if (m && fwrite(col, sizeof(int32_t), (size_t)m, fp.f) != (size_t)m) return GTAP_ERROR_INVALID_ARGUMENT;
+    return 0;
+}
+
 extern "C" int gtap_gen_tree(int32_t n, uint64_t seed, int32_t* left, int32_t* right, int32_t* value, int32_t* size) {
     if (n < 1 || !left || !right || !value || !size) return GTAP_ERROR_INVALID_ARGUMENT;
     std::mt19937_64 rng(seed);

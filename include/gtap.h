@@ -96,6 +96,22 @@ int gtap_gen_rmat(int32_t scale, int32_t edge_factor, uint64_t seed, int32_t* ro
 /* random unbalanced binary tree, 48% left split */
 int gtap_gen_tree(int32_t n, uint64_t seed, int32_t* left, int32_t* right, int32_t* value, int32_t* size);
 
+/* ------------------------------------------------------------------------ */
+/* the reference's input files, so its own datasets run when present        */
+/* ------------------------------------------------------------------------ */
+/* evaluation/util/gen_vector.c:21-60 (save_array / load_array): size_t n, then
+ * n int32.  out == NULL: *n_out only.  A file whose size disagrees with n, or
+ * capacity < n, is GTAP_ERROR_INVALID_ARGUMENT. */
+int gtap_read_array_file(const char* path, int32_t* out, int64_t capacity, int64_t* n_out);
+int gtap_write_array_file(const char* path, const int32_t* data, int64_t n);
+/* examples/asynchronous_bfs/asynchronous_bfs_thread.cu:69-84 (read_csr_binary):
+ * int N, int M, int row[N+1], int col[M].  row == col == NULL: sizes only.
+ * Offsets that do not run from 0 to M without decreasing, or a column outside
+ * [0, N), are GTAP_ERROR_INVALID_ARGUMENT. */
+int gtap_read_csr_file(const char* path, int32_t* row, int64_t row_capacity, int32_t* col, int64_t col_capacity,
+                       int32_t* n_out, int32_t* m_out);
+int gtap_write_csr_file(const char* path, const int32_t* row, const int32_t* col, int32_t n, int32_t m);
+
 /* Exactly-once stress test of the scheduler's deques and overflow queue on the
  * device (NEW, no reference counterpart): every warp publishes unique tokens
  * through the scheduler's own publish path and consumes them by pop, steal
