@@ -54,6 +54,50 @@ LOWERED_BUILDS = [
 ]
 
 
+PRAGMA_DIR = os.path.join(ROOT, "tests", "pragma")
+PRAGMA_BIN = os.path.join(PRAGMA_DIR, "bin")
+
+# Programs written with the gtap pragmas, lowered by gtap_b200.lower and then
+# compiled like the hand-lowered ones: (source, binary, -D settings).
+PRAGMA_BUILDS = [
+    ("fib_pragma.cu", "fib_pragma", "-DGTAP_GRID_SIZE=888 -DGTAP_BLOCK_SIZE=128 -DGTAP_MAX_CHILD_TASKS=2"),
+    ("nq_pragma.cu", "nq_pragma", "-DGTAP_GRID_SIZE=1184 -DGTAP_BLOCK_SIZE=128 -DGTAP_ASSUME_NO_TASKWAIT"),
+    ("cilksort_pragma.cu", "cilksort_pragma", "-DGTAP_GRID_SIZE=592 -DGTAP_BLOCK_SIZE=128 -DGTAP_MAX_CHILD_TASKS=4"),
+    ("tree_block_pragma.cu", "tree_block_pragma", "-DGTAP_GRID_SIZE=1184 -DGTAP_BLOCK_SIZE=128"),
+]
+
+
+def build_pragma(force=False):
+    """Lower and compile the pragma programs (tests/pragma/*.cu) against the
+    drop-in headers, linking libgtap_b200.so.  Returns the binaries' paths."""
+    from gtap_b200.lower import lower_source
+    build()
+    os.makedirs(PRAGMA_BIN, exist_ok=True)
+    nvcc = os.environ.get("NVCC", "nvcc")
+    header_deps = deps() + [os.path.join(HERE, "lower.py")]
+    outs = []
+    for src, name, defs in PRAGMA_BUILDS:
+        s = os.path.join(PRAGMA_DIR, src)
+        out = os.path.join(PRAGMA_BIN, name)
+        outs.append(out)
+        if (not force and os.path.exists(out)
+                and all(os.path.getmtime(p) <= os.path.getmtime(out) for p in header_deps + [s, LIB])):
+            continue
+        low = os.path.join(PRAGMA_BIN, name + "_lowered.cu")
+        with open(s) as f:
+            text = lower_source(f.read())
+        with open(low, "w") as f:
+            f.write(text)
+        cmd = ([nvcc, "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
+                "-diag-suppress", "550", "-I", os.path.join(ROOT, "include")] + defs.split()
+               + ["-o", out, low, "-L", HERE, "-lgtap_b200", "-Xlinker", "-rpath", "-Xlinker", "$ORIGIN/../../../gtap_b200"])
+        r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError("nvcc failed building %s" % name)
+    return outs
+
+
 def deps():
     out = []
     for d in (CSRC, os.path.join(ROOT, "include")):

@@ -1,0 +1,54 @@
+// fib_pragma.cu -- fib(n) written with the gtap pragmas (the source form the
+// reference's examples use), lowered by gtap_b200.lower before nvcc.
+//
+//   fib N CUTOFF REPS   prints one JSON line
+#include <stdio.h>
+#include <stdlib.h>
+#include <cuda_runtime.h>
+
+#include "gtap_thread.cuh"
+
+__device__ int d_result;
+__device__ int d_cutoff;
+
+__device__ int fib_serial(int n) { return n < 2 ? n : fib_serial(n - 1) + fib_serial(n - 2); }
+
+#pragma gtap function
+__device__ int fib(int n) {
+    if (n < 2) return n;
+    if (n < d_cutoff) return fib_serial(n);
+    int a, b;
+    #pragma gtap task
+    a = fib(n - 1);
+    #pragma gtap task
+    b = fib(n - 2);
+    #pragma gtap taskwait
+    return a + b;
+}
+
+__global__ void exec_kernel(int n) {
+    #pragma gtap entry
+    d_result = fib(n);
+}
+
+int main(int argc, char** argv) {
+    const int n = argc > 1 ? atoi(argv[1]) : 25;
+    const int cutoff = argc > 2 ? atoi(argv[2]) : 0;
+    const int reps = argc > 3 ? atoi(argv[3]) : 2;
+    cudaMemcpyToSymbol(d_cutoff, &cutoff, sizeof(int));
+    if (gtap_initialize() != cudaSuccess) return 1;
+    int result = -1;
+    printf("{\"program\": \"fib_pragma\", \"n\": %d, \"results\": [", n);
+    for (int r = 0; r < reps; ++r) {
+        if (r > 0 && gtap_reset() != cudaSuccess) return 1;
+        exec_kernel<<<GTAP_GRID_SIZE, GTAP_BLOCK_SIZE>>>(n);
+        if (gtap_synchronize() != cudaSuccess) return 1;
+        cudaMemcpyFromSymbol(&result, d_result, sizeof(int));
+        printf("%s%d", r ? ", " : "", result);
+    }
+    int code = 0;
+    gtap_get_runtime_error_code(&code);
+    printf("], \"error_code\": %d}\n", code);
+    gtap_finalize();
+    return code != 0;
+}

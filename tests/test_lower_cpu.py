@@ -1,0 +1,125 @@
+"""gtap_b200.lower on CPU: the pragma programs of tests/pragma lower to the
+task ABI and the result compiles for sm_100a against the drop-in headers;
+programs outside the supported subset are refused with a LoweringError."""
+import os
+import shutil
+import subprocess
+
+import pytest
+
+from gtap_b200.lower import LoweringError, lower_source
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PRAGMA = os.path.join(ROOT, "tests", "pragma")
+NVCC = os.environ.get("NVCC", "nvcc")
+
+
+def read(name):
+    with open(os.path.join(PRAGMA, name)) as f:
+        return f.read()
+
+
+def test_fib_lowers_to_a_state_machine():
+    out = lower_source(read("fib_pragma.cu"))
+    assert "#pragma gtap" not in out.replace("#pragma gtap function", "")   # every pragma was consumed
+    assert "struct __gtap_frame_fib" in out and "int __ret;" in out
+    assert "switch (__gtap_get_task_state(__tid))" in out
+    assert "__gtap_set_state_for_join(__tid, __cc, 1, 0)" in out
+    assert out.count("__gtap_spawn_task(") == 3           # two in fib, one in the entry task
+    assert "__gtap_release_task_id(__f->__child0)" in out
+    assert "const size_t __gtap_auto_task_data_size" in out
+    assert "__gtap_execute_task_loop_device();" in out
+
+
+def test_block_mode_follows_the_header():
+    out = lower_source(read("tree_block_pragma.cu"))
+    assert "__gtap_set_state_for_join_block(__tid, __ctx, 1, 0)" in out
+    assert "__syncthreads();" in out                      # child slots cleared before any thread spawns
+    assert "if (threadIdx.x == 0) __gtap_release_task_id" in out
+
+
+def test_only_live_locals_go_to_the_frame():
+    out = lower_source(read("nq_pragma.cu"))
+    frame = out[out.index("struct __gtap_frame_nq"):]
+    frame = frame[:frame.index("};")]
+    assert "avail" not in frame                           # no taskwait: nothing crosses one
+    out = lower_source(read("cilksort_pragma.cu"))
+    frame = out[out.index("struct __gtap_frame_csort"):]
+    frame = frame[:frame.index("};")]
+    assert "int h;" in frame and "int q1;" in frame       # used after the first taskwait
+
+
+BAD = {
+    "taskwait in a nested block": """
+#pragma gtap function
+__device__ void f(int n) {
+    if (n > 1) {
+        #pragma gtap task
+        f(n - 1);
+        #pragma gtap taskwait
+    }
+}
+""",
+    "result in a loop": """
+#pragma gtap function
+__device__ int f(int n) {
+    int s = 0;
+    for (int i = 0; i < n; ++i) {
+        #pragma gtap task
+        s = f(i);
+    }
+    #pragma gtap taskwait
+    return s;
+}
+""",
+    "task on a plain function": """
+__device__ int g(int n) { return n; }
+#pragma gtap function
+__device__ void f(int n) {
+    #pragma gtap task
+    g(n);
+}
+""",
+    "result without a taskwait": """
+#pragma gtap function
+__device__ int f(int n) {
+    int a;
+    #pragma gtap task
+    a = f(n - 1);
+    return a;
+}
+""",
+    "mixed declaration across a taskwait": """
+#pragma gtap function
+__device__ int f(int n) {
+    int a = n, b = 2;
+    #pragma gtap task
+    f(n - 1);
+    #pragma gtap taskwait
+    return a;
+}
+""",
+    "no task function": "__device__ int f(int n) { return n; }\n",
+}
+
+
+@pytest.mark.parametrize("what", sorted(BAD))
+def test_unsupported_programs_are_refused(what):
+    with pytest.raises(LoweringError):
+        lower_source(BAD[what])
+
+
+@pytest.mark.skipif(shutil.which(NVCC) is None, reason="nvcc not available")
+@pytest.mark.parametrize("src,defs", [
+    ("fib_pragma.cu", "-DGTAP_GRID_SIZE=888 -DGTAP_BLOCK_SIZE=128 -DGTAP_MAX_CHILD_TASKS=2"),
+    ("nq_pragma.cu", "-DGTAP_GRID_SIZE=1184 -DGTAP_BLOCK_SIZE=128 -DGTAP_ASSUME_NO_TASKWAIT"),
+    ("cilksort_pragma.cu", "-DGTAP_GRID_SIZE=592 -DGTAP_BLOCK_SIZE=128"),
+    ("tree_block_pragma.cu", "-DGTAP_GRID_SIZE=1184 -DGTAP_BLOCK_SIZE=128"),
+])
+def test_lowered_program_compiles(tmp_path, src, defs):
+    low = tmp_path / ("lowered_" + src)
+    low.write_text(lower_source(read(src)))
+    cmd = [NVCC, "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-diag-suppress", "550",
+           "-I", os.path.join(ROOT, "include"), "-c", str(low), "-o", str(tmp_path / "prog.o")] + defs.split()
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-3000:]
