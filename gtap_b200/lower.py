@@ -17,26 +17,32 @@ Pragmas
 Lowering (the contract of the reference's task ABI):
   * each task function becomes `void name__gtap_task(void*, int, TaskContext*)`
     with a frame struct `__gtap_frame_name` holding its parameters, the
-    locals declared at the top level of its body, the return value
-    (`__ret`) and one child id per spawn site whose result is used;
-  * the body is split at its taskwaits into the cases of a switch on
-    __gtap_get_task_state; a taskwait becomes __gtap_set_state_for_join
-    (thread mode) or __gtap_set_state_for_join_block (block mode) and returns
-    when children are outstanding;
+    locals that live across a taskwait, the return value (`__ret`) and one
+    child id per spawn site whose result is used;
+  * the body becomes one switch on __gtap_get_task_state; a taskwait becomes
+    __gtap_set_state_for_join (thread mode) or __gtap_set_state_for_join_block
+    (block mode), returning while children are outstanding, followed by the
+    case label the task resumes at -- inside the if/else branch that holds
+    the taskwait, if it is nested;
+  * a local in scope at a resume point moves to the frame when it is used
+    after that point or assigned a task's result; otherwise its initialiser
+    is split from its declaration, so no jump to a label crosses one;
   * a spawn becomes __gtap_spawn_task with the arguments written into the
     child's frame; a child whose result is assigned is retained, and its
     result is read from its frame, and its id released, right after the
-    taskwait that joins it;
+    taskwait that joins it (the left-hand side is evaluated there);
   * `return e;` stores e in the frame and calls __gtap_finish_task;
   * an entry pushes the root as task 0 (through a small entry task when its
     result is assigned) and runs __gtap_execute_task_loop_device.
 
-Restrictions (reported as LoweringError with the line):
-  * taskwaits at the top level of a task function's body (not inside if/for);
-  * locals that live across a taskwait declared at the top level of the body,
-    with builtin arithmetic or pointer types, no arrays, no shadowing;
-  * a spawn whose result is assigned is not inside a loop, and a taskwait
-    follows it;
+Restrictions (reported as LoweringError with the source line):
+  * no taskwait inside a loop or a switch, or as the body of an if/else
+    without braces; in block mode every thread of the block reaches it;
+  * locals that live across a taskwait have builtin arithmetic or pointer
+    types, are not arrays, and have a name no other local of the function
+    uses; no local shadows a parameter;
+  * a spawn whose result is assigned is not inside a loop, and the next
+    taskwait after it is in its own block or an enclosing one;
   * task functions are only called through `#pragma gtap task` / `entry`.
 """
 import argparse
@@ -195,9 +201,10 @@ def parse_params(text, line):
 
 
 class TaskFunction:
-    def __init__(self, name, ret, params, body, start, end, line):
+    def __init__(self, name, ret, params, body, start, end, line, body_line=None):
         self.name, self.ret, self.params, self.body = name, ret, params, body
         self.start, self.end, self.line = start, end, line
+        self.body_line = line if body_line is None else body_line   # source line of the body's first character
         self.locals = []        # [Param]
         self.child_slots = []   # names of child-id fields
 
@@ -233,7 +240,7 @@ def find_functions(src):
         bc = match_close(src, bo)
         funcs.append(TaskFunction(sig.group(3), " ".join(sig.group(2).split()),
                                   parse_params(src[po + 1:pc], line_of(src, po)), src[bo + 1:bc],
-                                  m.start(), bc + 1, line_of(src, m.start())))
+                                  m.start(), bc + 1, line_of(src, m.start()), line_of(src, bo + 1)))
     return funcs
 
 
@@ -278,6 +285,76 @@ DECL = re.compile(r"^\s*((?:(?:const|unsigned|signed|long|short|volatile)\s+)*"
                   r"(?:int|char|float|double|bool|size_t|u?int(?:8|16|32|64)_t|unsigned|long|short)\b[\s\*]*)(.*)$", re.S)
 
 
+GENERIC_DECL = re.compile(r"^\s*(?:(?:const|volatile|struct|static)\s+)*([A-Za-z_][\w:]*(?:\s*<[^;{}]*>)?)"
+                          r"[\s\*&]+([A-Za-z_]\w*)\s*(?:=|;|\[|,|\(|\{)")
+NOT_TYPES = {"return", "goto", "delete", "throw", "case", "else", "do", "typedef", "using", "break",
+             "continue", "new", "sizeof", "if", "for", "while", "switch", "asm"}
+CALL = re.compile(r"^(?:(?P<lhs>.+?)\s*=(?!=)\s*)?(?P<name>[A-Za-z_]\w*)\s*\((?P<args>.*)\)$", re.S)
+
+
+def _blocks(body):
+    """(open, close) of every brace pair in body (literals and comments skipped)."""
+    out, stack, j = [], [], 0
+    while j < len(body):
+        k = _skip_literal(body, j)
+        if k != j:
+            j = k
+            continue
+        if body[j] == "{":
+            stack.append(j)
+        elif body[j] == "}":
+            if not stack:
+                raise LoweringError("unbalanced '}' at line %d of a task function" % line_of(body, j))
+            out.append((stack.pop(), j))
+        j += 1
+    if stack:
+        raise LoweringError("unbalanced '{' at line %d of a task function" % line_of(body, stack[-1]))
+    return out
+
+
+def _header_kind(head):
+    """The control keyword whose header ends `head` (the text before a '{' or a
+    braceless statement): 'for', 'while', 'do', 'if', 'else', 'switch' or None."""
+    head = head.rstrip()
+    m = re.search(r"\b(do|else)$", head)
+    if m:
+        return m.group(1)
+    if not head.endswith(")"):
+        return None
+    depth, k = 0, len(head) - 1
+    while k >= 0:
+        if head[k] == ")":
+            depth += 1
+        elif head[k] == "(":
+            depth -= 1
+            if depth == 0:
+                break
+        k -= 1
+    m = re.search(r"\b(for|while|if|switch)\s*$", head[:max(k, 0)])
+    return m.group(1) if m else None
+
+
+def _declarators(m, line):
+    """[(name, stars, dims, init)] of a DECL match."""
+    out = []
+    for d in split_top(m.group(2).rstrip().rstrip(";")):
+        dm = re.match(r"^(\**)\s*([A-Za-z_]\w*)\s*((?:\[[^\]]*\]\s*)*)(?:=(.*))?$", d, re.S)
+        if not dm:
+            raise LoweringError("line %d: unsupported declaration '%s'" % (line, d))
+        out.append((dm.group(2), m.group(1).count("*") + len(dm.group(1)), dm.group(3).strip(),
+                    dm.group(4).strip() if dm.group(4) is not None else None))
+    return out
+
+
+def _local_type(m, stars):
+    """Type of a declarator: the declaration's base type plus its stars; a
+    top-level const is dropped (the variable is assigned after its declaration)."""
+    words = m.group(1).replace("*", " ").split()
+    if stars == 0:
+        words = [w for w in words if w != "const"]
+    return " ".join(words) + "*" * stars
+
+
 class Lowering:
     def __init__(self, src, mode):
         self.src, self.mode = src, mode
@@ -289,89 +366,157 @@ class Lowering:
 
     # -- task function body -------------------------------------------------
     def lower_function(self, f):
-        params = {p.name for p in f.params}
+        """One switch on the task state; each taskwait becomes a join that
+        returns while children are outstanding, followed by the case label the
+        task resumes at.  A taskwait may sit in nested if/else blocks, not in
+        a loop or a switch.  Locals in scope at a resume point either move to
+        the frame (when used after it, or assigned a task's result) or have
+        their initialiser split off, so no jump crosses an initialisation."""
         body = f.body
-        # split at the top-level taskwaits
-        segments, queues, last = [], [], 0
-        for s, e in top_level_statements(body):
-            pm = PRAGMA_AT.match(body, s)
-            if pm and pm.group(1) == "taskwait":
-                segments.append(body[last:s])
-                queues.append(parse_queue(pm.group(2), f.line))
-                last = e
-        segments.append(body[last:])
-        nested = [pm for pm in PRAGMA.finditer(body) if pm.group(1) == "taskwait"]
-        if len(nested) != len(queues):
-            raise LoweringError("line %d: a taskwait inside a nested block of '%s' is not supported"
-                                % (f.line, f.name))
-        # top-level declarations of each segment
-        decls, seen = [], set(params)
-        for i, seg in enumerate(segments):
-            for s, e in top_level_statements(seg):
-                st = seg[s:e]
-                m = DECL.match(st)
-                if not m or st.lstrip().startswith("#"):
+        params = {p.name for p in f.params}
+        blocks = _blocks(body)
+        whole = (-1, len(body))
+
+        def chain(pos):
+            return {b for b in blocks if b[0] < pos < b[1]}
+
+        def ln(pos):
+            # source line of a position in the original body
+            return f.body_line + body.count("\n", 0, pos)
+
+        prags = list(PRAGMA.finditer(body))
+        for pm in prags:
+            if pm.group(1) in ("function", "entry"):
+                raise LoweringError("line %d: '#pragma gtap %s' inside task function '%s'"
+                                    % (ln(pm.start()), pm.group(1), f.name))
+            if pm.group(1) not in ("task", "taskwait"):
+                raise LoweringError("line %d: unknown pragma '#pragma gtap %s'" % (ln(pm.start()), pm.group(1)))
+        waits = [pm for pm in prags if pm.group(1) == "taskwait"]
+        tasks = [pm for pm in prags if pm.group(1) == "task"]
+        for pm in waits:
+            before = body[:pm.start()]
+            if self._inside_loop(before):
+                raise LoweringError("line %d: a taskwait inside a loop of '%s' is not supported" % (ln(pm.start()), f.name))
+            if _header_kind(before) is not None:
+                raise LoweringError("line %d: a taskwait in '%s' is the body of an if/else without braces"
+                                    % (ln(pm.start()), f.name))
+            for o, _ in chain(pm.start()):
+                if _header_kind(body[:o]) == "switch":
+                    raise LoweringError("line %d: a taskwait inside a switch of '%s' is not supported"
+                                        % (ln(pm.start()), f.name))
+        # spawns whose result is assigned, and the taskwait that joins each
+        joins, lhs_idents = {}, set()
+        for ti, pm in enumerate(tasks):
+            call = body[pm.end():statement_end(body, pm.end())].strip()
+            m = CALL.match(call)
+            if not m or not m.group("lhs"):
+                continue
+            if self._inside_loop(body[:pm.start()]):
+                raise LoweringError("line %d: a task whose result is assigned is inside a loop" % ln(pm.start()))
+            nxt = next((k for k, w in enumerate(waits) if w.start() > pm.start()), None)
+            if nxt is None:
+                raise LoweringError("line %d: the result of a task in '%s' is assigned but no taskwait follows"
+                                    % (ln(pm.start()), f.name))
+            if not chain(waits[nxt].start()) <= chain(pm.start()):
+                raise LoweringError("line %d: the result of a task in '%s' is joined only inside a nested block"
+                                    % (ln(pm.start()), f.name))
+            joins[ti] = nxt
+            lhs_idents |= set(re.findall(r"[A-Za-z_]\w*", m.group("lhs")))
+        # declarations at the top level of every block
+        decls = []      # (start, end, block, match or None, [(name, stars, dims, init)])
+        for o, c in blocks + [whole]:
+            for s, e in top_level_statements(body[o + 1:c]):
+                s, e = s + o + 1, e + o + 1
+                st = body[s:e]
+                if st.lstrip().startswith("#"):
                     continue
-                base = " ".join(m.group(1).replace("*", " ").split())
-                names = []
-                for d in split_top(m.group(2).rstrip(";")):
-                    dm = re.match(r"^(\**)\s*([A-Za-z_]\w*)\s*(\[.*)?(=.*)?$", d, re.S)
-                    if not dm:
-                        raise LoweringError("line %d: unsupported declaration '%s'" % (f.line, d))
-                    if dm.group(2) in seen:
-                        raise LoweringError("line %d: '%s' declared twice" % (f.line, dm.group(2)))
-                    seen.add(dm.group(2))
-                    names.append((dm.group(2), base + "*" * (m.group(1).count("*") + len(dm.group(1))),
-                                  dm.group(3) is not None))
-                decls.append((i, names))
-        # a local lives in the frame when a later segment uses it, or when a
-        # task's result is assigned to it (the result is read after the join)
-        idents = [set(re.findall(r"[A-Za-z_]\w*", seg)) for seg in segments]
-        lhs_names = set()
-        for seg in segments:
-            for pm in PRAGMA.finditer(seg):
-                if pm.group(1) == "task":
-                    st = seg[pm.end():statement_end(seg, pm.end())]
-                    lm = re.match(r"^\s*([A-Za-z_]\w*)\s*=(?!=)", st)
-                    if lm:
-                        lhs_names.add(lm.group(1))
-        hoisted = set(params)
-        for i, names in decls:
-            live = [n for n, _, _ in names if n in lhs_names or any(n in idents[k] for k in range(i + 1, len(segments)))]
-            if live and len(live) != len(names):
-                raise LoweringError("line %d: declare '%s' (used after a taskwait) in a declaration of its own"
-                                    % (f.line, live[0]))
-            for n, ctype, is_array in names:
-                if n in live:
-                    if is_array:
-                        raise LoweringError("line %d: array '%s' cannot live across a taskwait" % (f.line, n))
-                    hoisted.add(n)
-                    f.locals.append(Param(ctype, n))
-        segments = [replace_identifiers(seg, hoisted) for seg in segments]
-        out_cases = []
-        pending = []   # spawns with results joined at the next taskwait: (slot, lhs, callee)
-        for i, seg in enumerate(segments):
-            seg, spawned = self.lower_segment(f, seg, i)
-            prologue = ""
-            for slot, lhs, callee in pending:
-                prologue += ("        if (__f->%s >= 0) {\n"
-                             "            %s = ((%s*)__gtap_get_task_data(__f->%s))->__ret;\n"
-                             "            %s__gtap_release_task_id(__f->%s);\n        }\n"
-                             % (slot, lhs, self.by_name[callee].frame, slot,
-                                "if (threadIdx.x == 0) " if self.mode == "block" else "", slot))
-            pending = spawned
-            if i < len(queues):
-                q = queues[i] or "0"
-                join = ("        if (__gtap_set_state_for_join_block(__tid, __ctx, %d, %s)) return;\n" % (i + 1, q)
-                        if self.mode == "block" else
-                        "        if (__gtap_set_state_for_join(__tid, __cc, %d, %s)) return;\n" % (i + 1, q))
-            else:
-                if pending:
-                    raise LoweringError("line %d: the result of a task in '%s' is assigned but no taskwait follows"
-                                        % (f.line, f.name))
-                join = "        __gtap_finish_task(__tid, __ctx);\n        return;\n"
-            out_cases.append("    case %d: {\n        int __cc = 0;\n        (void)__cc;\n%s%s\n%s    }\n"
-                             % (i, prologue, seg, join))
+                m = DECL.match(st)
+                if m:
+                    decls.append((s, e, (o, c), m, _declarators(m, ln(s))))
+                    continue
+                g = GENERIC_DECL.match(st)
+                if g and g.group(1) not in NOT_TYPES:
+                    decls.append((s, e, (o, c), None, [(g.group(2), 0, "", None)]))
+        hoist, count = {}, {}
+        for s, e, (o, c), m, names in decls:
+            crossing = [w for w in waits if e <= w.start() < c]
+            after = set()
+            for w in crossing:
+                after |= set(re.findall(r"[A-Za-z_]\w*", body[w.start():c]))
+            for name, stars, dims, init in names:
+                count[name] = count.get(name, 0) + 1
+                if name in params:
+                    raise LoweringError("line %d: local '%s' shadows a parameter of '%s'" % (ln(s), name, f.name))
+                if m is None:
+                    if crossing:
+                        raise LoweringError("line %d: local '%s' of '%s' has a type the lowering cannot keep "
+                                            "across a taskwait; declare it after the taskwait or in a block "
+                                            "that ends before it" % (ln(s), name, f.name))
+                    continue
+                if name in lhs_idents or (crossing and name in after):
+                    if dims:
+                        raise LoweringError("line %d: array '%s' cannot live across a taskwait" % (ln(s), name))
+                    hoist[name] = _local_type(m, stars)
+        for name in hoist:
+            if count[name] > 1:
+                raise LoweringError("line %d: '%s' is declared twice in '%s'; a local that lives across a "
+                                    "taskwait needs a name of its own" % (f.line, name, f.name))
+        # rewrite the declarations in scope at a resume point
+        edits = []
+        for s, e, (o, c), m, names in decls:
+            if m is None or not (any(e <= w.start() < c for w in waits) or any(n in hoist for n, _, _, _ in names)):
+                continue
+            parts = []
+            for name, stars, dims, init in names:
+                if name in hoist:
+                    if init is not None:
+                        parts.append("%s = %s;" % (name, init))
+                    continue
+                if dims and init is not None:
+                    raise LoweringError("line %d: array '%s' with an initialiser is in scope at a taskwait; "
+                                        "declare it after the taskwait" % (f.line, name))
+                parts.append("%s %s%s;" % (_local_type(m, stars), name, dims))
+                if init is not None:
+                    parts.append("%s = %s;" % (name, init))
+            edits.append((s, e, " ".join(parts)))
+        out, j = [], 0
+        for s, e, text in sorted(edits):
+            out.append(body[j:s])
+            out.append(text)
+            j = e
+        out.append(body[j:])
+        body = replace_identifiers("".join(out), params | set(hoist))
+        for n in hoist:
+            f.locals.append(Param(hoist[n], n))
+        body, at_wait = self.lower_spawns(f, body, joins)
+        body = self.lower_returns(f, body)
+        # taskwaits -> join + resume label + results of the joined children
+        out, j, k = [], 0, 0
+        for pm in PRAGMA.finditer(body):
+            if pm.group(1) != "taskwait":
+                continue
+            q = parse_queue(pm.group(2), f.line) or "0"
+            join = ("if (__gtap_set_state_for_join_block(__tid, __ctx, %d, %s)) return;" % (k + 1, q)
+                    if self.mode == "block" else
+                    "if (__gtap_set_state_for_join(__tid, __cc, %d, %s)) return;" % (k + 1, q))
+            results = ""
+            for slot, lhs, callee in at_wait.get(k, []):
+                results += ("        if (__f->%s >= 0) {\n"
+                            "            %s = ((%s*)__gtap_get_task_data(__f->%s))->__ret;\n"
+                            "            %s__gtap_release_task_id(__f->%s);\n        }\n"
+                            % (slot, lhs, self.by_name[callee].frame, slot,
+                               "if (threadIdx.x == 0) " if self.mode == "block" else "", slot))
+            out.append(body[j:body.index("#", pm.start())])
+            out.append("%s\n    case %d:\n        __cc = 0;\n%s" % (join, k + 1, results))
+            j = pm.end()
+            k += 1
+        out.append(body[j:])
+        body = "".join(out)
+        clears = "".join("__f->%s = -1; " % s for s in f.child_slots)
+        if clears:
+            # block mode: ordered before any thread of the block spawns
+            clears = ("        if (threadIdx.x == 0) { %s}\n        __syncthreads();\n" % clears if self.mode == "block"
+                      else "        %s\n" % clears)
         fields = ["    %s %s;" % (p.ctype, p.name) for p in f.params + f.locals]
         if f.ret != "void":
             fields.append("    %s __ret;" % f.ret)
@@ -382,27 +527,29 @@ class Lowering:
         fn = ("__device__ void %s(void* __frame, int __tid, TaskContext* __ctx) {\n"
               "    %s* __f = (%s*)__frame;\n"
               "    (void)__f;\n"
-              "    switch (__gtap_get_task_state(__tid)) {\n%s"
+              "    int __cc = 0;\n"
+              "    (void)__cc;\n"
+              "    switch (__gtap_get_task_state(__tid)) {\n"
+              "    case 0: {\n%s%s\n    }\n"
+              "        __gtap_finish_task(__tid, __ctx);\n        return;\n"
               "    default:\n        __gtap_finish_task(__tid, __ctx);\n        return;\n    }\n}\n"
-              % (f.task, f.frame, f.frame, "".join(out_cases)))
+              % (f.task, f.frame, f.frame, clears, body))
         return frame, fn
 
-    def lower_segment(self, f, seg, index):
-        """Rewrite spawns, top-level declarations and returns of one segment."""
-        spawned = []
-        # spawns
-        out, j = [], 0
-        for pm in list(PRAGMA.finditer(seg)):
-            if pm.group(1) in ("function", "entry"):
-                raise LoweringError("line %d: '#pragma gtap %s' inside task function '%s'"
-                                    % (f.line, pm.group(1), f.name))
+    def lower_spawns(self, f, body, joins):
+        """`#pragma gtap task [queue(q)]` + call -> __gtap_spawn_task with the
+        arguments written into the child's frame.  Returns the text and, per
+        taskwait index, the (slot, lhs, callee) of the results it joins."""
+        at_wait = {}
+        out, j, ti = [], 0, 0
+        for pm in list(PRAGMA.finditer(body)):
             if pm.group(1) != "task":
                 continue
             q = parse_queue(pm.group(2), f.line) or "0"
             s = pm.end()
-            e = statement_end(seg, s)
-            call = seg[s:e].strip()
-            m = re.match(r"^(?:(?P<lhs>.+?)\s*=(?!=)\s*)?(?P<name>[A-Za-z_]\w*)\s*\((?P<args>.*)\)$", call, re.S)
+            e = statement_end(body, s)
+            call = body[s:e].strip()
+            m = CALL.match(call)
             if not m or m.group("name") not in self.by_name:
                 raise LoweringError("line %d: '#pragma gtap task' must precede a call to a task function, got '%s'"
                                     % (f.line, call))
@@ -410,88 +557,50 @@ class Lowering:
             args = split_top(m.group("args"))
             if len(args) != len(callee.params):
                 raise LoweringError("line %d: '%s' takes %d arguments" % (f.line, callee.name, len(callee.params)))
-            before = seg[:pm.start()]
             lhs = m.group("lhs")
             if lhs and callee.ret == "void":
                 raise LoweringError("line %d: '%s' returns nothing" % (f.line, callee.name))
             if lhs:
-                if self._inside_loop(before):
-                    raise LoweringError("line %d: a task whose result is assigned is inside a loop" % f.line)
                 slot = "__child%d" % len(f.child_slots)
                 f.child_slots.append(slot)
-                spawned.append((slot, lhs, callee.name))
+                at_wait.setdefault(joins[ti], []).append((slot, lhs.strip(), callee.name))
                 tid_arg, retain = "&__f->" + slot, "true"
-                # the slot is cleared when the segment starts
             else:
                 tid_arg, retain = "nullptr", "false"
-            assign = "".join("            __c->%s = %s;\n" % (p.name, a) for p, a in zip(callee.params, args))
-            code = ("{\n            %s* __c = (%s*)__gtap_spawn_task(__ctx, __tid, &__cc, %s, %s, %s, %s);\n%s        }"
+            assign = "".join("        __c->%s = %s;\n" % (p.name, a) for p, a in zip(callee.params, args))
+            code = ("{\n        %s* __c = (%s*)__gtap_spawn_task(__ctx, __tid, &__cc, %s, %s, %s, %s);\n%s    }"
                     % (callee.frame, callee.frame, callee.task, q, tid_arg, retain, assign))
-            out.append(seg[j:pm.start()])
+            out.append(body[j:body.index("#", pm.start())])
             out.append(code)
             j = e + 1
-        out.append(seg[j:])
-        seg = "".join(out)
-        clears = "".join("__f->%s = -1; " % s for s, _, _ in spawned)
-        if clears:
-            # block mode: ordered before any thread of the block spawns
-            clears = ("        if (threadIdx.x == 0) { %s}\n        __syncthreads();\n" % clears if self.mode == "block"
-                      else "        %s\n" % clears)
-        # top-level declarations -> assignments
-        stmts = top_level_statements(seg)
+            ti += 1
+        out.append(body[j:])
+        return "".join(out), at_wait
+
+    def lower_returns(self, f, body):
+        """`return e;` -> the result into the frame, then __gtap_finish_task."""
         out, j = [], 0
-        for s, e in stmts:
-            st = seg[s:e]
-            m = DECL.match(st)
-            if m and not st.lstrip().startswith("#") and "__f->" in m.group(2).split("=")[0]:
-                # a hoisted declaration (all its names live in the frame)
-                assigns = []
-                for d in split_top(m.group(2).rstrip(";")):
-                    dm = re.match(r"^(\**)\s*(__f->[A-Za-z_]\w*)\s*(=(.*))?$", d, re.S)
-                    if dm and dm.group(3):
-                        assigns.append("%s = %s;" % (dm.group(2), dm.group(4).strip()))
-                out.append(seg[j:s])
-                out.append(" ".join(assigns))
-                j = e
-        out.append(seg[j:])
-        seg = "".join(out)
-        # returns
-        out, j = [], 0
-        for m in re.finditer(r"\breturn\b", seg):
+        for m in re.finditer(r"\breturn\b", body):
             if m.start() < j:
                 continue
-            e = statement_end(seg, m.end())
-            expr = seg[m.end():e].strip()
+            e = statement_end(body, m.end())
+            expr = body[m.end():e].strip()
             if expr:
                 if f.ret == "void":
                     raise LoweringError("line %d: '%s' returns void" % (f.line, f.name))
                 code = "{ __f->__ret = (%s); __gtap_finish_task(__tid, __ctx); return; }" % expr
             else:
                 code = "{ __gtap_finish_task(__tid, __ctx); return; }"
-            out.append(seg[j:m.start()])
+            out.append(body[j:m.start()])
             out.append(code)
             j = e + 1
-        out.append(seg[j:])
-        return clears + "".join(out), spawned
+        out.append(body[j:])
+        return "".join(out)
 
     @staticmethod
     def _loop_header(head):
         # head: the text before a '{' or a braceless statement; True if it ends a loop header
-        head = head.rstrip()
-        if re.search(r"\bdo$", head):
-            return True
-        if not head.endswith(")"):
-            return False
-        depth, k = 0, len(head) - 1
-        while k >= 0:
-            if head[k] == ")":
-                depth += 1
-            elif head[k] == "(":
-                depth -= 1
-                if depth == 0:
-                    break
-            k -= 1
-        return re.search(r"\b(for|while)\s*$", head[:max(k, 0)]) is not None
+        return _header_kind(head) in ("for", "while", "do")
 
     @classmethod
     def _inside_loop(cls, before):

@@ -36,6 +36,7 @@
 
 #include "gtap_types.h"
 #include "../gtap_b200/csrc/gtap_block_sched.cuh"
+#include "gtap_device_util.cuh"
 
 #ifndef GTAP_GRID_SIZE
 #define GTAP_GRID_SIZE 592

@@ -47,6 +47,7 @@
 
 #include "gtap_types.h"
 #include "../gtap_b200/csrc/gtap_thread_sched.cuh"
+#include "gtap_device_util.cuh"
 
 #ifndef GTAP_WARP_SIZE
 #define GTAP_WARP_SIZE 32

@@ -1,7 +1,8 @@
 // tree_block_pragma.cu -- a complete binary tree in block mode written with the
-// gtap pragmas: thread 0 forks both children with their results assigned, the
-// block waits, then every thread takes a share of the node's own work and the
-// node returns its value plus its children's.
+// gtap pragmas in the shape of the reference's block binary tree: the taskwait
+// sits in the else branch, thread 0 forks both children with their results
+// assigned, the block waits, then every thread takes a share of the node's own
+// work and the node returns its value plus its children's.
 //
 //   tree HEIGHT WORK   prints one JSON line
 #include <stdio.h>
@@ -28,17 +29,22 @@ __device__ unsigned long long node_value(int node, int work) {
 
 #pragma gtap function
 __device__ unsigned long long tree(int node, int height, int work) {
-    if (height == 0) return node_value(node, work);
     unsigned long long l = 0, r = 0;
-    if (threadIdx.x == 0) {
-        #pragma gtap task
-        l = tree(2 * node + 1, height - 1, work);
-        #pragma gtap task
-        r = tree(2 * node + 2, height - 1, work);
+    if (height == 0) {
+        return node_value(node, work);
+    } else {
+        if (threadIdx.x == 0) {
+            int lc = 2 * node + 1;
+            int rc = 2 * node + 2;
+            #pragma gtap task
+            l = tree(lc, height - 1, work);
+            #pragma gtap task
+            r = tree(rc, height - 1, work);
+        }
+        #pragma gtap taskwait
+        unsigned long long own = node_value(node, work);
+        return own + l + r;
     }
-    #pragma gtap taskwait
-    unsigned long long own = node_value(node, work);
-    return own + l + r;
 }
 
 __global__ void exec_kernel(int height, int work) {

@@ -1,7 +1,8 @@
 """Programs written with the gtap pragmas (tests/pragma), lowered by
 gtap_b200.lower and run on the B200 (B200 only): results must equal the
 oracle's (fib, n-queens), the sort must be ascending and a permutation of its
-input, and the block-mode tree sum must equal its closed form."""
+input, the block-mode tree sum must equal its closed form, and the ternary
+walk (taskwaits inside if/else branches) must equal its recursion in Python."""
 import json
 import os
 import subprocess
@@ -59,3 +60,35 @@ def test_tree_block_pragma(bins, height, work):
     r = run(bins["tree_block_pragma"], height, work)
     assert r["error_code"] == 0
     assert r["result"] == tree_expect(height, work)
+
+
+M64 = (1 << 64) - 1
+
+
+def walk_expect(depth, ident):
+    """walk_pragma.cu's walk() evaluated on the CPU, modulo 2^64."""
+    k = ident % 3
+    a = b = 0
+    own = ident
+    scale = depth * 7 + 1
+    if depth == 0:
+        return own * scale & M64
+    if k == 0:
+        a = walk_expect(depth - 1, 3 * ident + 1)
+        b = walk_expect(depth - 1, 3 * ident + 2)
+        own = (own + a - b) & M64
+    else:
+        own += ident & 7
+        if k == 1:
+            a = walk_expect(depth - 1, 3 * ident + 1)
+        walk_expect(depth - 1, 3 * ident + 2)
+        own = (own + 2 * a + k) & M64
+    b = walk_expect(depth // 2, ident + 1)
+    return (own * scale + b) & M64
+
+
+@pytest.mark.parametrize("depth,ident", [(0, 5), (1, 0), (1, 1), (1, 2), (6, 0), (9, 1), (11, 2), (16, 0), (16, 4)])
+def test_walk_pragma(bins, depth, ident):
+    r = run(bins["walk_pragma"], depth, ident)
+    assert r["error_code"] == 0
+    assert r["result"] == walk_expect(depth, ident)

@@ -49,15 +49,53 @@ def test_only_live_locals_go_to_the_frame():
     assert "int h;" in frame and "int q1;" in frame       # used after the first taskwait
 
 
+def test_taskwait_in_a_branch_resumes_inside_it():
+    out = lower_source(read("walk_pragma.cu"))
+    body = out[out.index("__device__ void walk__gtap_task(void* __frame, int __tid, TaskContext* __ctx) {"):]
+    # labels 1 and 2 sit in the two branches, 3 at the top level
+    assert body.index("case 1:") < body.index("} else {") < body.index("case 2:") < body.index("case 3:")
+    assert "int spare; spare = __f->id & 7;" in body           # in scope at a label, not used after it
+    assert "__f->k = __f->id % 3;" in body                     # const local kept in the frame
+    assert "__f->a = 0; __f->b = 0; __f->own = __f->id;" in body
+    assert "&__f->__child2, true" in body and "nullptr, false" in body
+    out = lower_source(read("tree_block_pragma.cu"))
+    assert "int lc = 2 * __f->node + 1;" in out                # declared in a block that ends before the join
+
+
 BAD = {
-    "taskwait in a nested block": """
+    "taskwait in a loop": """
 #pragma gtap function
 __device__ void f(int n) {
-    if (n > 1) {
+    for (int i = 0; i < n; ++i) {
+        #pragma gtap task
+        f(i);
+        #pragma gtap taskwait
+    }
+}
+""",
+    "taskwait in a switch": """
+#pragma gtap function
+__device__ void f(int n) {
+    switch (n) {
+    case 1: {
         #pragma gtap task
         f(n - 1);
         #pragma gtap taskwait
+        break;
     }
+    default:
+        break;
+    }
+}
+""",
+    "taskwait without braces": """
+#pragma gtap function
+__device__ void f(int n) {
+    #pragma gtap task
+    f(n - 1);
+    if (n > 2)
+        #pragma gtap taskwait
+    return;
 }
 """,
     "result in a loop": """
@@ -70,6 +108,18 @@ __device__ int f(int n) {
     }
     #pragma gtap taskwait
     return s;
+}
+""",
+    "result joined only in a branch": """
+#pragma gtap function
+__device__ int f(int n) {
+    int a = 0;
+    #pragma gtap task
+    a = f(n - 1);
+    if (n > 3) {
+        #pragma gtap taskwait
+    }
+    return a;
 }
 """,
     "task on a plain function": """
@@ -89,14 +139,52 @@ __device__ int f(int n) {
     return a;
 }
 """,
-    "mixed declaration across a taskwait": """
+    "live local declared twice": """
 #pragma gtap function
 __device__ int f(int n) {
-    int a = n, b = 2;
+    int a = 0;
+    if (n > 1) {
+        #pragma gtap task
+        a = f(n - 1);
+        #pragma gtap taskwait
+    } else {
+        int a = 1;
+        return a;
+    }
+    return a;
+}
+""",
+    "local shadows a parameter": """
+#pragma gtap function
+__device__ void f(int n) {
+    if (n > 1) {
+        int n = 3;
+        #pragma gtap task
+        f(n - 1);
+    }
+}
+""",
+    "class-type local across a taskwait": """
+struct P { int x; };
+#pragma gtap function
+__device__ void f(int n) {
+    P p;
+    p.x = n;
     #pragma gtap task
     f(n - 1);
     #pragma gtap taskwait
-    return a;
+    n = p.x;
+}
+""",
+    "array live across a taskwait": """
+#pragma gtap function
+__device__ void f(int n) {
+    int v[4];
+    v[0] = n;
+    #pragma gtap task
+    f(n - 1);
+    #pragma gtap taskwait
+    n = v[0];
 }
 """,
     "no task function": "__device__ int f(int n) { return n; }\n",
@@ -115,6 +203,7 @@ def test_unsupported_programs_are_refused(what):
     ("nq_pragma.cu", "-DGTAP_GRID_SIZE=1184 -DGTAP_BLOCK_SIZE=128 -DGTAP_ASSUME_NO_TASKWAIT"),
     ("cilksort_pragma.cu", "-DGTAP_GRID_SIZE=592 -DGTAP_BLOCK_SIZE=128"),
     ("tree_block_pragma.cu", "-DGTAP_GRID_SIZE=1184 -DGTAP_BLOCK_SIZE=128"),
+    ("walk_pragma.cu", "-DGTAP_GRID_SIZE=888 -DGTAP_BLOCK_SIZE=128"),
 ])
 def test_lowered_program_compiles(tmp_path, src, defs):
     low = tmp_path / ("lowered_" + src)
