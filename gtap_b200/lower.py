@@ -30,10 +30,16 @@ Lowering (the contract of the reference's task ABI):
   * a spawn becomes __gtap_spawn_task with the arguments written into the
     child's frame; a child whose result is assigned is retained, and its
     result is read from its frame, and its id released, right after the
-    taskwait that joins it (the left-hand side is evaluated there);
+    taskwait that joins it (the left-hand side is evaluated there); a local
+    that only receives results of unconditional spawns joined at one
+    taskwait, and is read only before the next one, stays a plain local;
   * `return e;` stores e in the frame and calls __gtap_finish_task;
   * an entry pushes the root as task 0 (through a small entry task when its
-    result is assigned) and runs __gtap_execute_task_loop_device.
+    result is assigned) and runs __gtap_execute_task_loop_device;
+  * the output starts with `#define GTAP_DIRECT_DISPATCH 1` and defines
+    __gtap_dispatch, which the drop-in headers call to run a task: the stored
+    function pointer is compared with each task function and the match is
+    called directly, so the bodies are inlined into the worker loop.
 
 Restrictions (reported as LoweringError with the source line):
   * no taskwait inside a loop or a switch, or as the body of an if/else
@@ -207,6 +213,7 @@ class TaskFunction:
         self.body_line = line if body_line is None else body_line   # source line of the body's first character
         self.locals = []        # [Param]
         self.child_slots = []   # names of child-id fields
+        self.cond_slots = []    # those whose spawn may not run before its join
 
     @property
     def frame(self):
@@ -346,6 +353,32 @@ def _declarators(m, line):
     return out
 
 
+def _is_written(text, name):
+    """True if `name` (not as a member) is assigned, incremented or has its
+    address taken anywhere in text."""
+    j = 0
+    ident = re.compile(r"[A-Za-z_]\w*")
+    while j < len(text):
+        k = _skip_literal(text, j)
+        if k != j:
+            j = k
+            continue
+        m = ident.match(text, j)
+        if not m:
+            j += 1
+            continue
+        if m.group(0) == name:
+            before = text[:m.start()].rstrip()
+            after = text[m.end():]
+            if not (before.endswith(".") or before.endswith("->")):
+                if re.match(r"\s*(?:<<|>>|[-+*/%&|^])?=(?!=)", after) or re.match(r"\s*(?:\+\+|--)", after):
+                    return True
+                if re.search(r"(?:\+\+|--)$", before) or (before.endswith("&") and not before.endswith("&&")):
+                    return True
+        j = m.end()
+    return False
+
+
 def _local_type(m, stars):
     """Type of a declarator: the declaration's base type plus its stars; a
     top-level const is dropped (the variable is assigned after its declaration)."""
@@ -405,7 +438,8 @@ class Lowering:
                     raise LoweringError("line %d: a taskwait inside a switch of '%s' is not supported"
                                         % (ln(pm.start()), f.name))
         # spawns whose result is assigned, and the taskwait that joins each
-        joins, lhs_idents = {}, set()
+        joins, cond, lhs_idents = {}, {}, set()
+        bare = {}       # bare identifier on the left -> [(task index, start, end of the spawn statement)]
         for ti, pm in enumerate(tasks):
             call = body[pm.end():statement_end(body, pm.end())].strip()
             m = CALL.match(call)
@@ -421,7 +455,11 @@ class Lowering:
                 raise LoweringError("line %d: the result of a task in '%s' is joined only inside a nested block"
                                     % (ln(pm.start()), f.name))
             joins[ti] = nxt
+            # conditional: the spawn sits in a block the taskwait is not in
+            cond[ti] = chain(waits[nxt].start()) != chain(pm.start())
             lhs_idents |= set(re.findall(r"[A-Za-z_]\w*", m.group("lhs")))
+            if re.match(r"^[A-Za-z_]\w*$", m.group("lhs").strip()):
+                bare.setdefault(m.group("lhs").strip(), []).append((ti, pm.start(), statement_end(body, pm.end())))
         # declarations at the top level of every block
         decls = []      # (start, end, block, match or None, [(name, stars, dims, init)])
         for o, c in blocks + [whole]:
@@ -437,6 +475,33 @@ class Lowering:
                 g = GENERIC_DECL.match(st)
                 if g and g.group(1) not in NOT_TYPES:
                     decls.append((s, e, (o, c), None, [(g.group(2), 0, "", None)]))
+        # result-only locals: assigned the results of unconditional spawns
+        # joined at one taskwait and read only between that taskwait and the
+        # next.  The join always overwrites them, so they stay plain locals
+        # and the frame stays small.
+        result_only = set()
+        for name, sites in bare.items():
+            ks = {joins[ti] for ti, _, _ in sites}
+            if len(ks) != 1 or any(cond[ti] for ti, _, _ in sites) or name in params:
+                continue
+            k = ks.pop()
+            mine = [d for d in decls if any(n == name for n, _, _, _ in d[4])]
+            if len(mine) != 1 or mine[0][3] is None:
+                continue
+            ds, de, (o, c), _, names = mine[0]
+            if any(n == name and dims for n, _, dims, _ in names) or not (o < waits[k].start() < c):
+                continue
+            lo = waits[k].end()
+            hi = waits[k + 1].start() if k + 1 < len(waits) else len(body)
+            ok = True
+            for um in re.finditer(r"\b%s\b" % re.escape(name), body):
+                u = um.start()
+                if ds <= u < de or any(a <= u <= b for _, a, b in sites) or lo <= u < hi:
+                    continue
+                ok = False
+                break
+            if ok:
+                result_only.add(name)
         hoist, count = {}, {}
         for s, e, (o, c), m, names in decls:
             crossing = [w for w in waits if e <= w.start() < c]
@@ -453,7 +518,7 @@ class Lowering:
                                             "across a taskwait; declare it after the taskwait or in a block "
                                             "that ends before it" % (ln(s), name, f.name))
                     continue
-                if name in lhs_idents or (crossing and name in after):
+                if name not in result_only and (name in lhs_idents or (crossing and name in after)):
                     if dims:
                         raise LoweringError("line %d: array '%s' cannot live across a taskwait" % (ln(s), name))
                     hoist[name] = _local_type(m, stars)
@@ -485,10 +550,12 @@ class Lowering:
             out.append(text)
             j = e
         out.append(body[j:])
-        body = replace_identifiers("".join(out), params | set(hoist))
+        # parameters the body never writes are read from the frame once, on entry
+        readonly = [p for p in f.params if not _is_written(f.body, p.name)]
+        body = replace_identifiers("".join(out), (params - {p.name for p in readonly}) | set(hoist))
         for n in hoist:
             f.locals.append(Param(hoist[n], n))
-        body, at_wait = self.lower_spawns(f, body, joins)
+        body, at_wait = self.lower_spawns(f, body, joins, cond)
         body = self.lower_returns(f, body)
         # taskwaits -> join + resume label + results of the joined children
         out, j, k = [], 0, 0
@@ -499,20 +566,23 @@ class Lowering:
             join = ("if (__gtap_set_state_for_join_block(__tid, __ctx, %d, %s)) return;" % (k + 1, q)
                     if self.mode == "block" else
                     "if (__gtap_set_state_for_join(__tid, __cc, %d, %s)) return;" % (k + 1, q))
-            results = ""
-            for slot, lhs, callee in at_wait.get(k, []):
-                results += ("        if (__f->%s >= 0) {\n"
-                            "            %s = ((%s*)__gtap_get_task_data(__f->%s))->__ret;\n"
-                            "            %s__gtap_release_task_id(__f->%s);\n        }\n"
-                            % (slot, lhs, self.by_name[callee].frame, slot,
-                               "if (threadIdx.x == 0) " if self.mode == "block" else "", slot))
+            # every result is read before any id is released, so the reads
+            # overlap; an unconditional spawn always ran before this join
+            reads, releases = "", ""
+            for slot, lhs, callee, conditional in at_wait.get(k, []):
+                guard = "if (__f->%s >= 0) " % slot if conditional else ""
+                reads += ("        %s%s = ((%s*)__gtap_get_task_data(__f->%s))->__ret;\n"
+                          % (guard, lhs, self.by_name[callee].frame, slot))
+                releases += ("        %s%s__gtap_release_task_id(__f->%s);\n"
+                             % (guard, "if (threadIdx.x == 0) " if self.mode == "block" else "", slot))
+            results = reads + releases
             out.append(body[j:body.index("#", pm.start())])
             out.append("%s\n    case %d:\n        __cc = 0;\n%s" % (join, k + 1, results))
             j = pm.end()
             k += 1
         out.append(body[j:])
         body = "".join(out)
-        clears = "".join("__f->%s = -1; " % s for s in f.child_slots)
+        clears = "".join("__f->%s = -1; " % s for s in f.cond_slots)
         if clears:
             # block mode: ordered before any thread of the block spawns
             clears = ("        if (threadIdx.x == 0) { %s}\n        __syncthreads();\n" % clears if self.mode == "block"
@@ -527,16 +597,19 @@ class Lowering:
         fn = ("__device__ void %s(void* __frame, int __tid, TaskContext* __ctx) {\n"
               "    %s* __f = (%s*)__frame;\n"
               "    (void)__f;\n"
+              "%s"
               "    int __cc = 0;\n"
               "    (void)__cc;\n"
               "    switch (__gtap_get_task_state(__tid)) {\n"
               "    case 0: {\n%s%s\n    }\n"
               "        __gtap_finish_task(__tid, __ctx);\n        return;\n"
               "    default:\n        __gtap_finish_task(__tid, __ctx);\n        return;\n    }\n}\n"
-              % (f.task, f.frame, f.frame, clears, body))
+              % (f.task, f.frame, f.frame,
+                 "".join("    %s %s = __f->%s;\n    (void)%s;\n" % (p.ctype, p.name, p.name, p.name) for p in readonly),
+                 clears, body))
         return frame, fn
 
-    def lower_spawns(self, f, body, joins):
+    def lower_spawns(self, f, body, joins, cond):
         """`#pragma gtap task [queue(q)]` + call -> __gtap_spawn_task with the
         arguments written into the child's frame.  Returns the text and, per
         taskwait index, the (slot, lhs, callee) of the results it joins."""
@@ -563,7 +636,9 @@ class Lowering:
             if lhs:
                 slot = "__child%d" % len(f.child_slots)
                 f.child_slots.append(slot)
-                at_wait.setdefault(joins[ti], []).append((slot, lhs.strip(), callee.name))
+                at_wait.setdefault(joins[ti], []).append((slot, lhs.strip(), callee.name, cond[ti]))
+                if cond[ti]:
+                    f.cond_slots.append(slot)   # cleared on entry: the spawn may not run
                 tid_arg, retain = "&__f->" + slot, "true"
             else:
                 tid_arg, retain = "nullptr", "false"
@@ -707,8 +782,16 @@ class Lowering:
         size_expr = "sizeof(%s)" % sizes[0]
         for s in sizes[1:]:
             size_expr = "(sizeof(%s) > %s ? sizeof(%s) : %s)" % (s, size_expr, s, size_expr)
-        # entry tasks and the frame size follow the last task function
-        tail = "".join(self.entry_defs) + "const size_t __gtap_auto_task_data_size = %s;\n" % size_expr
+        # entry tasks, the direct dispatch and the frame size follow the last task function
+        tasks = [f.task for f in self.funcs] + ["__gtap_entry%d" % k for k in range(len(self.entry_defs))]
+        dispatch = ("__device__ void __gtap_dispatch(unsigned long long __fn, void* __frame, int __tid, "
+                    "TaskContext* __ctx) {\n"
+                    + "".join("    if (__fn == (unsigned long long)(void*)&%s) { %s(__frame, __tid, __ctx); return; }\n"
+                              % (t, t) for t in tasks)
+                    + "    ((void (*)(void*, int, TaskContext*))__fn)(__frame, __tid, __ctx);   // a task not lowered here\n"
+                    "}\n")
+        tail = ("".join(self.entry_defs) + dispatch
+                + "const size_t __gtap_auto_task_data_size = %s;\n" % size_expr)
         pieces, j = [], 0
         for k, f in enumerate(funcs):
             pieces.append(src[j:f.start])
@@ -719,7 +802,9 @@ class Lowering:
                 pieces.append(tail)
             j = f.end
         pieces.append(src[j:])
-        return "".join(pieces)
+        # before any include: the drop-in headers then call the task functions
+        # through __gtap_dispatch instead of an indirect call
+        return "#define GTAP_DIRECT_DISPATCH 1\n" + "".join(pieces)
 
 
 def lower_source(src, mode=None):

@@ -70,6 +70,16 @@ const char* gtap_get_runtime_error_string(int error_code);
 // The per-block scheduler state task code receives and passes back; opaque.
 struct TaskContext;
 
+// Programs that define GTAP_DIRECT_DISPATCH before including this header
+// provide __gtap_dispatch (gtap_b200.lower emits it): it compares the stored
+// function pointer with each task function of the program and calls the match
+// directly, so the task bodies are inlined into the worker loop instead of
+// being reached by an indirect call (which cannot be inlined and saves its
+// registers to the stack on every call).
+#ifdef GTAP_DIRECT_DISPATCH
+__device__ void __gtap_dispatch(unsigned long long fn, void* frame, int tid, TaskContext* ctx);
+#endif
+
 // Largest task frame in bytes, defined by the lowered program
 // (reference runtime/detail/common/gtap_runtime_common.cuh:9).
 extern const size_t __gtap_auto_task_data_size;
@@ -95,8 +105,12 @@ struct Program {
     __device__ static bool root_args_ok(const gtap_root&) { return true; }
     __device__ static void init_root(const gtap::Arena&, const gtap_root&, void*) {}
     __device__ static void exec(const gtap::Arena& A, gtap::BlockShared& S, int tid, int*) {
+#ifdef GTAP_DIRECT_DISPATCH
+        __gtap_dispatch(S.fn, gtap::frame_of(A, tid), tid, reinterpret_cast<TaskContext*>(&S));
+#else
         using Fn = void (*)(void*, int, TaskContext*);
         reinterpret_cast<Fn>(S.fn)(gtap::frame_of(A, tid), tid, reinterpret_cast<TaskContext*>(&S));
+#endif
     }
 };
 

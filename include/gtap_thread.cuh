@@ -100,6 +100,16 @@ int gtap_visualize_profile(const char* app_name);
 // The per-warp scheduler state task code receives and passes back; opaque.
 struct TaskContext;
 
+// Programs that define GTAP_DIRECT_DISPATCH before including this header
+// provide __gtap_dispatch (gtap_b200.lower emits it): it compares the stored
+// function pointer with each task function of the program and calls the match
+// directly, so the task bodies are inlined into the worker loop instead of
+// being reached by an indirect call (which cannot be inlined and saves its
+// registers to the stack on every call).
+#ifdef GTAP_DIRECT_DISPATCH
+__device__ void __gtap_dispatch(unsigned long long fn, void* frame, int tid, TaskContext* ctx);
+#endif
+
 // Largest task frame in bytes, defined by the lowered program
 // (reference runtime/detail/common/gtap_runtime_common.cuh:9).
 extern const size_t __gtap_auto_task_data_size;
@@ -145,8 +155,12 @@ struct Program {
                                        const int4&) {}
     __device__ static void exec(const gtap::Arena&, gtap::WarpShared& S, int, int tid, void* frame, const int4&,
                                 const int4&, unsigned long long fn) {
+#ifdef GTAP_DIRECT_DISPATCH
+        __gtap_dispatch(fn, frame, tid, reinterpret_cast<TaskContext*>(&S));
+#else
         using Fn = void (*)(void*, int, TaskContext*);
         reinterpret_cast<Fn>(fn)(frame, tid, reinterpret_cast<TaskContext*>(&S));
+#endif
     }
 };
 

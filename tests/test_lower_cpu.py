@@ -29,6 +29,9 @@ def test_fib_lowers_to_a_state_machine():
     assert "__gtap_release_task_id(__f->__child0)" in out
     assert "const size_t __gtap_auto_task_data_size" in out
     assert "__gtap_execute_task_loop_device();" in out
+    assert out.startswith("#define GTAP_DIRECT_DISPATCH 1\n")
+    assert "if (__fn == (unsigned long long)(void*)&fib__gtap_task) { fib__gtap_task(__frame, __tid, __ctx); return; }" in out
+    assert "(void*)&__gtap_entry0)" in out
 
 
 def test_block_mode_follows_the_header():
@@ -36,6 +39,19 @@ def test_block_mode_follows_the_header():
     assert "__gtap_set_state_for_join_block(__tid, __ctx, 1, 0)" in out
     assert "__syncthreads();" in out                      # child slots cleared before any thread spawns
     assert "if (threadIdx.x == 0) __gtap_release_task_id" in out
+
+
+def test_result_only_locals_stay_out_of_the_frame():
+    out = lower_source(read("fib_pragma.cu"))
+    frame = out[out.index("struct __gtap_frame_fib"):]
+    frame = frame[:frame.index("};")]
+    # a and b only receive the children's results at the one taskwait
+    assert frame.split() == ["struct", "__gtap_frame_fib", "{", "int", "n;", "int", "__ret;",
+                             "int", "__child0;", "int", "__child1;"]
+    body = out[out.index("__device__ void fib__gtap_task(void* __frame, int __tid, TaskContext* __ctx) {"):]
+    # both results are read before either id is released
+    assert (body.index("b = ((__gtap_frame_fib*)__gtap_get_task_data(__f->__child1))->__ret;")
+            < body.index("__gtap_release_task_id(__f->__child0);"))
 
 
 def test_only_live_locals_go_to_the_frame():
@@ -54,12 +70,16 @@ def test_taskwait_in_a_branch_resumes_inside_it():
     body = out[out.index("__device__ void walk__gtap_task(void* __frame, int __tid, TaskContext* __ctx) {"):]
     # labels 1 and 2 sit in the two branches, 3 at the top level
     assert body.index("case 1:") < body.index("} else {") < body.index("case 2:") < body.index("case 3:")
-    assert "int spare; spare = __f->id & 7;" in body           # in scope at a label, not used after it
-    assert "__f->k = __f->id % 3;" in body                     # const local kept in the frame
-    assert "__f->a = 0; __f->b = 0; __f->own = __f->id;" in body
+    assert "int spare; spare = id & 7;" in body                # in scope at a label, not used after it
+    assert "__f->k = id % 3;" in body                          # const local kept in the frame
+    assert "__f->a = 0; __f->b = 0; __f->own = id;" in body
+    assert "    int id = __f->id;\n" in body                     # parameters never written: read once
     assert "&__f->__child2, true" in body and "nullptr, false" in body
+    # a conditional spawn's slot is cleared on entry and checked at its join
+    assert "__f->__child2 = -1; " in body and "if (__f->__child2 >= 0) __f->a =" in body
+    assert "__f->__child0 = -1" not in body
     out = lower_source(read("tree_block_pragma.cu"))
-    assert "int lc = 2 * __f->node + 1;" in out                # declared in a block that ends before the join
+    assert "int lc = 2 * node + 1;" in out                     # declared in a block that ends before the join
 
 
 BAD = {
