@@ -34,6 +34,13 @@ def test_fib_pragma(bins, n, cutoff):
     assert r["results"] == [orc.fib(n)] * 2
 
 
+@pytest.mark.parametrize("n,cutoff", [(0, 0), (2, 0), (22, 0), (29, 0), (32, 14)])
+def test_fib_queues_pragma(bins, n, cutoff):
+    r = run(bins["fib_queues_pragma"], n, cutoff, 2)
+    assert r["error_code"] == 0 and r["queues"] == 3
+    assert r["results"] == [orc.fib(n)] * 2
+
+
 @pytest.mark.parametrize("n,cutoff", [(4, 3), (8, 7), (10, 4), (12, 6)])
 def test_nq_pragma(bins, n, cutoff):
     r = run(bins["nq_pragma"], n, cutoff)

@@ -34,6 +34,13 @@ def test_fib_lowers_to_a_state_machine():
     assert "(void*)&__gtap_entry0)" in out
 
 
+def test_queue_clauses_reach_the_runtime_calls():
+    out = lower_source(read("fib_queues_pragma.cu"))
+    assert "fib__gtap_task, (n - 1) & 1, &__f->__child0, true)" in out
+    assert "fib__gtap_task, n & 1, &__f->__child1, true)" in out
+    assert "__gtap_set_state_for_join(__tid, __cc, 1, 2)" in out
+
+
 def test_block_mode_follows_the_header():
     out = lower_source(read("tree_block_pragma.cu"))
     assert "__gtap_set_state_for_join_block(__tid, __ctx, 1, 0)" in out
@@ -224,6 +231,7 @@ def test_unsupported_programs_are_refused(what):
     ("cilksort_pragma.cu", "-DGTAP_GRID_SIZE=592 -DGTAP_BLOCK_SIZE=128"),
     ("tree_block_pragma.cu", "-DGTAP_GRID_SIZE=1184 -DGTAP_BLOCK_SIZE=128"),
     ("walk_pragma.cu", "-DGTAP_GRID_SIZE=888 -DGTAP_BLOCK_SIZE=128"),
+    ("fib_queues_pragma.cu", "-DGTAP_GRID_SIZE=888 -DGTAP_BLOCK_SIZE=128 -DGTAP_NUM_QUEUES=3"),
 ])
 def test_lowered_program_compiles(tmp_path, src, defs):
     low = tmp_path / ("lowered_" + src)
