@@ -65,6 +65,8 @@ PRAGMA_BUILDS = [
     ("cilksort_pragma.cu", "cilksort_pragma", "-DGTAP_GRID_SIZE=592 -DGTAP_BLOCK_SIZE=128 -DGTAP_MAX_CHILD_TASKS=4"),
     ("tree_block_pragma.cu", "tree_block_pragma", "-DGTAP_GRID_SIZE=1184 -DGTAP_BLOCK_SIZE=128"),
     ("walk_pragma.cu", "walk_pragma", "-DGTAP_GRID_SIZE=888 -DGTAP_BLOCK_SIZE=128"),
+    ("bary_tree_pragma.cu", "bary_tree_pragma",
+     "-DGTAP_GRID_SIZE=888 -DGTAP_BLOCK_SIZE=128 -DGTAP_MAX_CHILD_TASKS=8"),
     ("fib_queues_pragma.cu", "fib_queues_pragma",
      "-DGTAP_GRID_SIZE=888 -DGTAP_BLOCK_SIZE=128 -DGTAP_MAX_CHILD_TASKS=2 -DGTAP_NUM_QUEUES=3"),
 ]

@@ -7,6 +7,7 @@
  */
 #include "oracle.h"
 
+#include <math.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -457,4 +458,63 @@ int64_t orc_seq_root(int kind, int param, uint64_t seed) {
     free(a);
     free(t);
     return ok;
+}
+
+/* ---- probabilistic B-ary tree (gtap_thread_tree_load_compute.cu:96-143) -- */
+uint32_t orc_fmix32(uint32_t h) {
+    h ^= h >> 16;
+    h *= 0x85ebca6bu;
+    h ^= h >> 13;
+    h *= 0xc2b2ae35u;
+    h ^= h >> 16;
+    return h;
+}
+
+void orc_bary_input(uint64_t seed, double* out, int64_t n) {
+    uint64_t x = seed;
+    for (int64_t i = 0; i < n; ++i) {
+        x += 0x9e3779b97f4a7c15ull;
+        uint64_t z = x;
+        z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+        z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+        z ^= z >> 31;
+        out[i] = (double)(z >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+    }
+}
+
+uint32_t orc_bary_node_work(uint32_t node, const double* input, int64_t n, int mem_ops, int iters) {
+    const uint32_t seed = orc_fmix32(node ^ 0x2545f491u);
+    double acc = 0.0;
+    for (int m = 0; m < mem_ops; ++m) acc += input[orc_fmix32(seed + (uint32_t)m) & (uint32_t)(n - 1)];
+    uint32_t mix = (seed ^ 0x9e3779b9u) + (uint32_t)(int32_t)acc;
+    double y = 0.0;
+    for (int it = 0; it < iters; ++it) {
+        const double x = (double)orc_fmix32(seed + (uint32_t)it * 0x632be5abu);
+        y = fma(x, 1.0000001192092896, y);
+        uint64_t bits;
+        memcpy(&bits, &y, sizeof(bits));
+        mix ^= (uint32_t)bits ^ (uint32_t)(bits >> 32);
+    }
+    return mix;
+}
+
+static void bary_rec(uint32_t node, int d, int D, int B, int mem_ops, int iters, const double* input, int64_t n,
+                     uint64_t* sum, int64_t* nodes) {
+    if (d < D) {
+        uint32_t s = orc_fmix32(node ^ ((uint32_t)d * 0x9e3779b9u));
+        for (int k = 0; k < B; ++k) {
+            s = orc_fmix32(s + (uint32_t)k);
+            if ((int)(s % (uint32_t)D) < D - d)
+                bary_rec(node * (uint32_t)B + (uint32_t)(k + 1), d + 1, D, B, mem_ops, iters, input, n, sum, nodes);
+        }
+    }
+    *sum += orc_bary_node_work(node, input, n, mem_ops, iters);
+    *nodes += 1;
+}
+
+void orc_bary_tree(int depth_max, int branch, int mem_ops, int iters, const double* input, int64_t n,
+                   uint64_t* sum, int64_t* nodes) {
+    *sum = 0;
+    *nodes = 0;
+    bary_rec(0u, 0, depth_max, branch, mem_ops, iters, input, n, sum, nodes);
 }

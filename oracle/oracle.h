@@ -98,6 +98,22 @@ int64_t orc_seq_root(int kind, int param, uint64_t seed);
 /* seq_cilksort.cpp:50-69 on caller-provided keys (no key generation inside). */
 void orc_seq_cilksort(int32_t* arr, int32_t* tmp, int64_t n);
 
+/* ---- probabilistic B-ary tree ------------------------------------------- *
+ * The workload shape of evaluation/2-comparison/prob_Bary_tree/
+ * gtap_thread_tree_load_compute.cu:96-143: a node at depth d < D keeps each
+ * of its B child candidates with probability 1 - d/D, drawn from a hash of
+ * the node id; every node does seeded loads of a double array and a loop of
+ * fused multiply-adds after its children finish.  Here each node's work ends
+ * in a 32-bit mix that is summed over all nodes (a deterministic result, where
+ * the reference's own program only stores into a racy sink).  Hash: the
+ * MurmurHash3 32-bit finaliser; input: splitmix64 (Steele, Lea, Flood 2014)
+ * mapped to doubles in [-1, 1). */
+uint32_t orc_fmix32(uint32_t h);
+void orc_bary_input(uint64_t seed, double* out, int64_t n);
+uint32_t orc_bary_node_work(uint32_t node, const double* input, int64_t n, int mem_ops, int iters);
+void orc_bary_tree(int depth_max, int branch, int mem_ops, int iters, const double* input, int64_t n,
+                   uint64_t* sum, int64_t* nodes);
+
 #ifdef __cplusplus
 }
 #endif

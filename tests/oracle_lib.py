@@ -41,6 +41,10 @@ def load():
             "orc_root_mix": (None, [u64, i32, vp, vp, vp]),
             "orc_seq_root": (i64, [ctypes.c_int, ctypes.c_int, u64]),
             "orc_seq_cilksort": (None, [vp, vp, i64]),
+            "orc_fmix32": (u32, [u32]),
+            "orc_bary_input": (None, [u64, vp, i64]),
+            "orc_bary_node_work": (u32, [u32, vp, i64, ctypes.c_int, ctypes.c_int]),
+            "orc_bary_tree": (None, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, i64, vp, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -142,3 +146,17 @@ def root_mix(seed, n):
     ks = np.empty(n, np.uint64)
     load().orc_root_mix(seed, n, p(kind), p(param), p(ks))
     return kind, param, ks
+
+
+def bary_input(seed, n):
+    out = np.empty(n, dtype=np.float64)
+    load().orc_bary_input(seed, p(out), n)
+    return out
+
+
+def bary_tree(depth_max, branch, mem_ops, iters, inp):
+    """(sum of the nodes' 32-bit mixes mod 2^64, node count) of the probabilistic B-ary tree."""
+    s = np.zeros(1, dtype=np.uint64)
+    c = np.zeros(1, dtype=np.int64)
+    load().orc_bary_tree(depth_max, branch, mem_ops, iters, p(inp), len(inp), p(s), p(c))
+    return int(s[0]), int(c[0])

@@ -2,7 +2,8 @@
 gtap_b200.lower and run on the B200 (B200 only): results must equal the
 oracle's (fib, n-queens), the sort must be ascending and a permutation of its
 input, the block-mode tree sum must equal its closed form, and the ternary
-walk (taskwaits inside if/else branches) must equal its recursion in Python."""
+walk (taskwaits inside if/else branches) must equal its recursion in Python;
+the probabilistic B-ary tree's mix sum and node count must equal the oracle's."""
 import json
 import os
 import subprocess
@@ -99,3 +100,16 @@ def test_walk_pragma(bins, depth, ident):
     r = run(bins["walk_pragma"], depth, ident)
     assert r["error_code"] == 0
     assert r["result"] == walk_expect(depth, ident)
+
+
+@pytest.mark.parametrize("D,B,mem_ops,iters,log2n", [
+    (0, 3, 4, 4, 10), (1, 3, 4, 4, 10), (6, 3, 8, 16, 12), (9, 4, 16, 32, 16), (15, 4, 8, 8, 16),
+    (18, 4, 16, 64, 22),
+])
+def test_bary_tree_pragma(bins, D, B, mem_ops, iters, log2n):
+    seed = 7 + D
+    r = run(bins["bary_tree_pragma"], D, B, mem_ops, iters, log2n, seed, 2)
+    assert r["error_code"] == 0
+    total, nodes = orc.bary_tree(D, B, mem_ops, iters, orc.bary_input(seed, 1 << log2n))
+    assert r["nodes"] == nodes
+    assert r["sum"] == total
