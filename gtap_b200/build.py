@@ -67,6 +67,7 @@ PRAGMA_BUILDS = [
     ("walk_pragma.cu", "walk_pragma", "-DGTAP_GRID_SIZE=888 -DGTAP_BLOCK_SIZE=128"),
     ("bary_tree_pragma.cu", "bary_tree_pragma",
      "-DGTAP_GRID_SIZE=888 -DGTAP_BLOCK_SIZE=128 -DGTAP_MAX_CHILD_TASKS=8"),
+    ("bary_block_pragma.cu", "bary_block_pragma", "-DGTAP_GRID_SIZE=1184 -DGTAP_BLOCK_SIZE=128"),
     ("fib_queues_pragma.cu", "fib_queues_pragma",
      "-DGTAP_GRID_SIZE=888 -DGTAP_BLOCK_SIZE=128 -DGTAP_MAX_CHILD_TASKS=2 -DGTAP_NUM_QUEUES=3"),
 ]

@@ -498,17 +498,40 @@ uint32_t orc_bary_node_work(uint32_t node, const double* input, int64_t n, int m
     return mix;
 }
 
-static void bary_rec(uint32_t node, int d, int D, int B, int mem_ops, int iters, const double* input, int64_t n,
-                     uint64_t* sum, int64_t* nodes) {
+uint32_t orc_bary_node_work_block(uint32_t node, const double* input, int64_t n, int mem_ops, int iters, int threads) {
+    const uint32_t seed = orc_fmix32(node ^ 0x2545f491u);
+    double acc = 0.0;
+    uint32_t xr = 0;
+    for (int t = 0; t < threads; ++t) {
+        double part = 0.0;
+        for (int m = t; m < mem_ops; m += threads) part += input[orc_fmix32(seed + (uint32_t)m) & (uint32_t)(n - 1)];
+        acc += part;
+        double y = 0.0;
+        for (int it = t; it < iters; it += threads) {
+            const double x = (double)orc_fmix32(seed + (uint32_t)it * 0x632be5abu);
+            y = fma(x, 1.0000001192092896, y);
+            uint64_t bits;
+            memcpy(&bits, &y, sizeof(bits));
+            xr ^= (uint32_t)bits ^ (uint32_t)(bits >> 32);
+        }
+    }
+    return ((seed ^ 0x9e3779b9u) + (uint32_t)(int32_t)acc) ^ xr;
+}
+
+/* threads == 0: thread mode (orc_bary_node_work), else block mode with that many threads */
+static void bary_rec(uint32_t node, int d, int D, int B, int mem_ops, int iters, int threads, const double* input,
+                     int64_t n, uint64_t* sum, int64_t* nodes) {
     if (d < D) {
         uint32_t s = orc_fmix32(node ^ ((uint32_t)d * 0x9e3779b9u));
         for (int k = 0; k < B; ++k) {
             s = orc_fmix32(s + (uint32_t)k);
             if ((int)(s % (uint32_t)D) < D - d)
-                bary_rec(node * (uint32_t)B + (uint32_t)(k + 1), d + 1, D, B, mem_ops, iters, input, n, sum, nodes);
+                bary_rec(node * (uint32_t)B + (uint32_t)(k + 1), d + 1, D, B, mem_ops, iters, threads, input, n, sum,
+                         nodes);
         }
     }
-    *sum += orc_bary_node_work(node, input, n, mem_ops, iters);
+    *sum += threads ? orc_bary_node_work_block(node, input, n, mem_ops, iters, threads)
+                    : orc_bary_node_work(node, input, n, mem_ops, iters);
     *nodes += 1;
 }
 
@@ -516,5 +539,12 @@ void orc_bary_tree(int depth_max, int branch, int mem_ops, int iters, const doub
                    uint64_t* sum, int64_t* nodes) {
     *sum = 0;
     *nodes = 0;
-    bary_rec(0u, 0, depth_max, branch, mem_ops, iters, input, n, sum, nodes);
+    bary_rec(0u, 0, depth_max, branch, mem_ops, iters, 0, input, n, sum, nodes);
+}
+
+void orc_bary_tree_block(int depth_max, int branch, int mem_ops, int iters, int threads, const double* input,
+                         int64_t n, uint64_t* sum, int64_t* nodes) {
+    *sum = 0;
+    *nodes = 0;
+    bary_rec(0u, 0, depth_max, branch, mem_ops, iters, threads < 1 ? 1 : threads, input, n, sum, nodes);
 }

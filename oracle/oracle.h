@@ -113,6 +113,13 @@ void orc_bary_input(uint64_t seed, double* out, int64_t n);
 uint32_t orc_bary_node_work(uint32_t node, const double* input, int64_t n, int mem_ops, int iters);
 void orc_bary_tree(int depth_max, int branch, int mem_ops, int iters, const double* input, int64_t n,
                    uint64_t* sum, int64_t* nodes);
+/* Block mode (gtap_block_tree_load_compute.cu): the same tree, each node's
+ * work split over the T threads of a block -- thread t takes loads m = t,
+ * t+T, ... and fma steps it = t, t+T, ... in order; the T partial sums are
+ * added in thread order and the T xor-words combined. */
+uint32_t orc_bary_node_work_block(uint32_t node, const double* input, int64_t n, int mem_ops, int iters, int threads);
+void orc_bary_tree_block(int depth_max, int branch, int mem_ops, int iters, int threads, const double* input,
+                         int64_t n, uint64_t* sum, int64_t* nodes);
 
 #ifdef __cplusplus
 }

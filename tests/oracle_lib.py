@@ -45,6 +45,9 @@ def load():
             "orc_bary_input": (None, [u64, vp, i64]),
             "orc_bary_node_work": (u32, [u32, vp, i64, ctypes.c_int, ctypes.c_int]),
             "orc_bary_tree": (None, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, i64, vp, vp]),
+            "orc_bary_node_work_block": (u32, [u32, vp, i64, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+            "orc_bary_tree_block": (None, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, i64,
+                                           vp, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -159,4 +162,12 @@ def bary_tree(depth_max, branch, mem_ops, iters, inp):
     s = np.zeros(1, dtype=np.uint64)
     c = np.zeros(1, dtype=np.int64)
     load().orc_bary_tree(depth_max, branch, mem_ops, iters, p(inp), len(inp), p(s), p(c))
+    return int(s[0]), int(c[0])
+
+
+def bary_tree_block(depth_max, branch, mem_ops, iters, threads, inp):
+    """bary_tree with each node's work split over a block of `threads` threads."""
+    s = np.zeros(1, dtype=np.uint64)
+    c = np.zeros(1, dtype=np.int64)
+    load().orc_bary_tree_block(depth_max, branch, mem_ops, iters, threads, p(inp), len(inp), p(s), p(c))
     return int(s[0]), int(c[0])

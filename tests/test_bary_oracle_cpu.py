@@ -101,3 +101,34 @@ def test_spawn_probability_follows_depth():
     for d in range(D):
         if tried[d] >= 200:
             assert abs(kept[d] / tried[d] - (D - d) / D) < 0.08
+
+
+def node_work_block(node, inp, mem_ops, iters, threads):
+    seed = fmix32(node ^ 0x2545F491)
+    acc, xr = 0.0, 0
+    for t in range(threads):
+        part = 0.0
+        for m in range(t, mem_ops, threads):
+            part += float(inp[fmix32((seed + m) & M32) & (len(inp) - 1)])
+        acc += part
+        y = 0.0
+        for it in range(t, iters, threads):
+            y = fma(float(fmix32((seed + it * 0x632BE5AB) & M32)), 1.0000001192092896, y)
+            bits = struct.unpack("<Q", struct.pack("<d", y))[0]
+            xr ^= (bits & M32) ^ (bits >> 32)
+    return (((seed ^ 0x9E3779B9) + (int(acc) & M32)) & M32) ^ xr
+
+
+def test_block_node_work_matches_exact_restatement():
+    inp = orc.bary_input(5, 1 << 12)
+    L = orc.load()
+    for node in [0, 9, 77777, M32]:
+        for mem_ops, iters, threads in [(0, 0, 32), (5, 3, 4), (300, 200, 128), (64, 512, 128)]:
+            assert (L.orc_bary_node_work_block(node, orc.p(inp), len(inp), mem_ops, iters, threads)
+                    == node_work_block(node, inp, mem_ops, iters, threads))
+
+
+def test_block_tree_has_the_thread_tree_shape():
+    inp = orc.bary_input(9, 1 << 10)
+    for D, B in [(0, 2), (5, 3), (8, 4)]:
+        assert orc.bary_tree_block(D, B, 4, 4, 32, inp)[1] == orc.bary_tree(D, B, 4, 4, inp)[1]

@@ -3,7 +3,8 @@ gtap_b200.lower and run on the B200 (B200 only): results must equal the
 oracle's (fib, n-queens), the sort must be ascending and a permutation of its
 input, the block-mode tree sum must equal its closed form, and the ternary
 walk (taskwaits inside if/else branches) must equal its recursion in Python;
-the probabilistic B-ary tree's mix sum and node count must equal the oracle's."""
+the probabilistic B-ary tree's mix sum and node count must equal the oracle's,
+in thread mode and in block mode."""
 import json
 import os
 import subprocess
@@ -111,5 +112,17 @@ def test_bary_tree_pragma(bins, D, B, mem_ops, iters, log2n):
     r = run(bins["bary_tree_pragma"], D, B, mem_ops, iters, log2n, seed, 2)
     assert r["error_code"] == 0
     total, nodes = orc.bary_tree(D, B, mem_ops, iters, orc.bary_input(seed, 1 << log2n))
+    assert r["nodes"] == nodes
+    assert r["sum"] == total
+
+
+@pytest.mark.parametrize("D,B,mem_ops,iters,log2n", [
+    (0, 3, 4, 4, 10), (1, 3, 300, 200, 10), (6, 3, 64, 256, 12), (9, 4, 300, 200, 16), (13, 4, 128, 512, 20),
+])
+def test_bary_block_pragma(bins, D, B, mem_ops, iters, log2n):
+    seed = 11 + D
+    r = run(bins["bary_block_pragma"], D, B, mem_ops, iters, log2n, seed, 2)
+    assert r["error_code"] == 0
+    total, nodes = orc.bary_tree_block(D, B, mem_ops, iters, r["threads"], orc.bary_input(seed, 1 << log2n))
     assert r["nodes"] == nodes
     assert r["sum"] == total

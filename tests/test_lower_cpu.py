@@ -233,6 +233,7 @@ def test_unsupported_programs_are_refused(what):
     ("walk_pragma.cu", "-DGTAP_GRID_SIZE=888 -DGTAP_BLOCK_SIZE=128"),
     ("fib_queues_pragma.cu", "-DGTAP_GRID_SIZE=888 -DGTAP_BLOCK_SIZE=128 -DGTAP_NUM_QUEUES=3"),
     ("bary_tree_pragma.cu", "-DGTAP_GRID_SIZE=888 -DGTAP_BLOCK_SIZE=128 -DGTAP_MAX_CHILD_TASKS=8"),
+    ("bary_block_pragma.cu", "-DGTAP_GRID_SIZE=1184 -DGTAP_BLOCK_SIZE=128"),
 ])
 def test_lowered_program_compiles(tmp_path, src, defs):
     low = tmp_path / ("lowered_" + src)
