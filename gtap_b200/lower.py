@@ -353,6 +353,25 @@ def _declarators(m, line):
     return out
 
 
+def _words(text, word):
+    """Matches of the identifier `word` outside string/char literals and comments."""
+    out, j = [], 0
+    ident = re.compile(r"[A-Za-z_]\w*")
+    while j < len(text):
+        k = _skip_literal(text, j)
+        if k != j:
+            j = k
+            continue
+        m = ident.match(text, j)
+        if not m:
+            j += 1
+            continue
+        if m.group(0) == word:
+            out.append(m)
+        j = m.end()
+    return out
+
+
 def _is_written(text, name):
     """True if `name` (not as a member) is assigned, incremented or has its
     address taken anywhere in text."""
@@ -445,6 +464,9 @@ class Lowering:
             m = CALL.match(call)
             if not m or not m.group("lhs"):
                 continue
+            if re.search(r"[-+*/%&|^<>!]$", m.group("lhs").strip()):
+                raise LoweringError("line %d: a task's result can only be assigned with '=', not '%s='"
+                                    % (ln(pm.start()), m.group("lhs").strip().split()[-1][-1]))
             if self._inside_loop(body[:pm.start()]):
                 raise LoweringError("line %d: a task whose result is assigned is inside a loop" % ln(pm.start()))
             nxt = next((k for k, w in enumerate(waits) if w.start() > pm.start()), None)
@@ -655,7 +677,7 @@ class Lowering:
     def lower_returns(self, f, body):
         """`return e;` -> the result into the frame, then __gtap_finish_task."""
         out, j = [], 0
-        for m in re.finditer(r"\breturn\b", body):
+        for m in _words(body, "return"):
             if m.start() < j:
                 continue
             e = statement_end(body, m.end())

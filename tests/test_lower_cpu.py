@@ -215,6 +215,16 @@ __device__ void f(int n) {
 }
 """,
     "no task function": "__device__ int f(int n) { return n; }\n",
+    "compound assignment of a result": """
+#pragma gtap function
+__device__ int f(int n) {
+    int a = 0;
+    #pragma gtap task
+    a += f(n - 1);
+    #pragma gtap taskwait
+    return a;
+}
+""",
 }
 
 
@@ -240,5 +250,92 @@ def test_lowered_program_compiles(tmp_path, src, defs):
     low.write_text(lower_source(read(src)))
     cmd = [NVCC, "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-diag-suppress", "550",
            "-I", os.path.join(ROOT, "include"), "-c", str(low), "-o", str(tmp_path / "prog.o")] + defs.split()
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-3000:]
+
+
+EDGE = {
+    # braces and `return` inside comments and string literals stay as written
+    "comments_strings": """
+#include <stdio.h>
+#include "gtap_thread.cuh"
+#pragma gtap function
+__device__ int f(int n) {
+    // a comment with { braces and return 3;
+    if (n < 2) { /* } closing brace in a comment */ return n; }
+    int a, b;
+    #pragma gtap task
+    a = f(n - 1);   // trailing comment }
+    #pragma gtap task
+    b = f(n - 2);
+    #pragma gtap taskwait
+    if (n == 99) printf("{ return %d; }\\n", a);
+    return a + b;
+}
+""",
+    # taskwaits in an else-if chain, a result assigned to the function's own local
+    "else_if": """
+#include "gtap_thread.cuh"
+#pragma gtap function
+__device__ int f(int n) {
+    int r = 0;
+    if (n < 2) {
+        return n;
+    } else if (n % 2 == 0) {
+        int a, b;
+        #pragma gtap task
+        a = f(n - 1);
+        #pragma gtap task
+        b = f(n - 2);
+        #pragma gtap taskwait
+        r = a + b;
+    } else {
+        int c;
+        #pragma gtap task
+        c = f(n - 1);
+        #pragma gtap task
+        r = f(n - 2);
+        #pragma gtap taskwait
+        r += c;
+    }
+    return r;
+}
+""",
+    # a declaration initialised by a spawn
+    "decl_init": """
+#include "gtap_thread.cuh"
+#pragma gtap function
+__device__ int f(int n) {
+    if (n < 2) return n;
+    #pragma gtap task
+    int a = f(n - 1);
+    #pragma gtap taskwait
+    return a;
+}
+""",
+}
+
+
+def test_literals_and_comments_are_kept():
+    out = lower_source(EDGE["comments_strings"])
+    assert "// a comment with { braces and return 3;" in out
+    assert "/* } closing brace in a comment */" in out
+    assert 'printf("{ return %d; }\\n", ' in out
+
+
+def test_else_if_chain_resumes_in_each_branch():
+    out = lower_source(EDGE["else_if"])
+    body = out[out.index("__device__ void f__gtap_task(void* __frame, int __tid, TaskContext* __ctx) {"):]
+    assert body.index("} else if (n % 2 == 0) {") < body.index("case 1:") < body.index("} else {") < body.index("case 2:")
+
+
+@pytest.mark.skipif(shutil.which(NVCC) is None, reason="nvcc not available")
+@pytest.mark.parametrize("name", sorted(EDGE))
+def test_edge_programs_compile(tmp_path, name):
+    low = tmp_path / (name + ".cu")
+    low.write_text(lower_source(EDGE[name]))
+    cmd = [NVCC, "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-diag-suppress", "550",
+           "-I", os.path.join(ROOT, "include"), "-DGTAP_GRID_SIZE=888", "-DGTAP_BLOCK_SIZE=128",
+           "-c", str(low), "-o", str(tmp_path / "prog.o")]
     r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-3000:]
