@@ -62,7 +62,12 @@ def parse():
 
 
 def algorithmic_bytes(mix, results):
-    """Bytes per step the algorithm must move (roofline)."""
+    """Bytes per step the algorithm must move.  fib tasks: the parent's argument
+    write and the child's read of a frame, the deque slot write and read, the
+    join-counter update and the result read.  n-queens tasks (no join): the
+    frame write and read and the deque slot.  cilksort roots: each task's
+    frame, deque slot and join counter, plus 8 bytes per key (a 4-byte read
+    and write) for the leaf pass and for two merge passes per four-way level."""
     total = 0
     for i, r in enumerate(results):
         k = int(mix.kind[i])
