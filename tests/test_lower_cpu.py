@@ -339,3 +339,23 @@ def test_edge_programs_compile(tmp_path, name):
            "-c", str(low), "-o", str(tmp_path / "prog.o")]
     r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-3000:]
+
+
+def test_command_line(tmp_path):
+    import sys
+    out = tmp_path / "fib_lowered.cu"
+    r = subprocess.run([sys.executable, "-m", "gtap_b200.lower", os.path.join(PRAGMA, "fib_pragma.cu"), "-o", str(out)],
+                       cwd=ROOT, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    assert out.read_text() == lower_source(read("fib_pragma.cu"))
+    bad = tmp_path / "bad.cu"
+    bad.write_text(BAD["taskwait in a loop"])
+    r = subprocess.run([sys.executable, "-m", "gtap_b200.lower", str(bad), "-o", str(tmp_path / "x.cu")],
+                       cwd=ROOT, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 1
+    assert "line 7: a taskwait inside a loop of 'f' is not supported" in r.stderr
+    assert not (tmp_path / "x.cu").exists()
+    # --mode overrides the header the program includes
+    r = subprocess.run([sys.executable, "-m", "gtap_b200.lower", os.path.join(PRAGMA, "fib_pragma.cu"), "-o",
+                        str(out), "--mode", "block"], cwd=ROOT, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and "__gtap_set_state_for_join_block" in out.read_text()
