@@ -408,8 +408,11 @@ def _local_type(m, stars):
 
 
 class Lowering:
-    def __init__(self, src, mode):
-        self.src, self.mode = src, mode
+    def __init__(self, src, mode, results="retain"):
+        self.src, self.mode, self.results = src, mode, results
+        self.parent = results == "parent"
+        if self.parent and mode != "thread":
+            raise LoweringError("--results parent needs thread mode")
         self.funcs = find_functions(src)
         self.by_name = {f.name: f for f in self.funcs}
         self.entries = 0
@@ -482,6 +485,8 @@ class Lowering:
             lhs_idents |= set(re.findall(r"[A-Za-z_]\w*", m.group("lhs")))
             if re.match(r"^[A-Za-z_]\w*$", m.group("lhs").strip()):
                 bare.setdefault(m.group("lhs").strip(), []).append((ti, pm.start(), statement_end(body, pm.end())))
+        if self.parent:
+            self._check_parent_results(f, body, tasks, waits, joins, bare, ln)
         # declarations at the top level of every block
         decls = []      # (start, end, block, match or None, [(name, stars, dims, init)])
         for o, c in blocks + [whole]:
@@ -502,7 +507,7 @@ class Lowering:
         # next.  The join always overwrites them, so they stay plain locals
         # and the frame stays small.
         result_only = set()
-        for name, sites in bare.items():
+        for name, sites in ([] if self.parent else bare.items()):
             ks = {joins[ti] for ti, _, _ in sites}
             if len(ks) != 1 or any(cond[ti] for ti, _, _ in sites) or name in params:
                 continue
@@ -548,6 +553,18 @@ class Lowering:
             if count[name] > 1:
                 raise LoweringError("line %d: '%s' is declared twice in '%s'; a local that lives across a "
                                     "taskwait needs a name of its own" % (f.line, name, f.name))
+        if self.parent:
+            types = dict(hoist)
+            types.update({p.name: " ".join(p.ctype.split()) for p in f.params})
+            for name, sites in bare.items():
+                for ti, a, _ in sites:
+                    callee = self.by_name[CALL.match(body[tasks[ti].end():statement_end(body, tasks[ti].end())]
+                                                     .strip()).group("name")]
+                    if types.get(name) != callee.ret:
+                        raise LoweringError("line %d: with --results parent, '%s' must be a local or parameter of "
+                                            "type '%s' (the return type of '%s')" % (ln(a), name, callee.ret,
+                                                                                     callee.name))
+            f.targets = sorted(set(bare))
         # rewrite the declarations in scope at a resume point
         edits = []
         for s, e, (o, c), m, names in decls:
@@ -579,6 +596,9 @@ class Lowering:
             f.locals.append(Param(hoist[n], n))
         body, at_wait = self.lower_spawns(f, body, joins, cond)
         body = self.lower_returns(f, body)
+        # with --results parent the task works on a copy of its frame: write
+        # it back before a join that may suspend it
+        writeback = "*__fm = *__f; " if self.parent else ""
         # taskwaits -> join + resume label + results of the joined children
         out, j, k = [], 0, 0
         for pm in PRAGMA.finditer(body):
@@ -587,7 +607,7 @@ class Lowering:
             q = parse_queue(pm.group(2), f.line) or "0"
             join = ("if (__gtap_set_state_for_join_block(__tid, __ctx, %d, %s)) return;" % (k + 1, q)
                     if self.mode == "block" else
-                    "if (__gtap_set_state_for_join(__tid, __cc, %d, %s)) return;" % (k + 1, q))
+                    "%sif (__gtap_set_state_for_join(__tid, __cc, %d, %s)) return;" % (writeback, k + 1, q))
             # every result is read before any id is released, so the reads
             # overlap; an unconditional spawn always ran before this join
             reads, releases = "", ""
@@ -611,11 +631,17 @@ class Lowering:
                       else "        %s\n" % clears)
         fields = ["    %s %s;" % (p.ctype, p.name) for p in f.params + f.locals]
         if f.ret != "void":
-            fields.append("    %s __ret;" % f.ret)
+            # parent mode: where the result goes (0: nowhere), else the result itself
+            fields.append("    unsigned __dst;" if self.parent else "    %s __ret;" % f.ret)
         fields += ["    int %s;" % s for s in f.child_slots]
         if not fields:
             fields = ["    int __unused;"]
         frame = "struct %s {\n%s\n};\n" % (f.frame, "\n".join(fields))
+        if self.parent:
+            frame += "".join("static_assert(offsetof(%s, %s) %% 4 == 0 && offsetof(%s, %s) < 128, "
+                             "\"a task result is delivered into the first 128 bytes of the frame\");\n"
+                             % (f.frame, t, f.frame, t) for t in getattr(f, "targets", []))
+            return frame, self._parent_function(f, readonly, body)
         fn = ("__device__ void %s(void* __frame, int __tid, TaskContext* __ctx) {\n"
               "    %s* __f = (%s*)__frame;\n"
               "    (void)__f;\n"
@@ -655,6 +681,19 @@ class Lowering:
             lhs = m.group("lhs")
             if lhs and callee.ret == "void":
                 raise LoweringError("line %d: '%s' returns nothing" % (f.line, callee.name))
+            if self.parent:
+                assign = "".join("        __c->%s = %s;\n" % (p.name, a) for p, a in zip(callee.params, args))
+                if callee.ret != "void":
+                    field = lhs.strip()[len("__f->"):] if lhs else None
+                    assign += ("        __c->__dst = __gtap_dst(__tid, offsetof(%s, %s));\n" % (f.frame, field)
+                               if lhs else "        __c->__dst = 0u;\n")
+                code = ("{\n        %s* __c = (%s*)__gtap_spawn_task(__ctx, __tid, &__cc, %s, %s, nullptr, false);\n%s    }"
+                        % (callee.frame, callee.frame, callee.task, q, assign))
+                out.append(body[j:body.index("#", pm.start())])
+                out.append(code)
+                j = e + 1
+                ti += 1
+                continue
             if lhs:
                 slot = "__child%d" % len(f.child_slots)
                 f.child_slots.append(slot)
@@ -685,7 +724,9 @@ class Lowering:
             if expr:
                 if f.ret == "void":
                     raise LoweringError("line %d: '%s' returns void" % (f.line, f.name))
-                code = "{ __f->__ret = (%s); __gtap_finish_task(__tid, __ctx); return; }" % expr
+                code = ("{ if (__f->__dst) __gtap_deliver<%s>(__f->__dst, (%s)); __gtap_finish_task(__tid, __ctx); return; }"
+                        % (f.ret, expr) if self.parent else
+                        "{ __f->__ret = (%s); __gtap_finish_task(__tid, __ctx); return; }" % expr)
             else:
                 code = "{ __gtap_finish_task(__tid, __ctx); return; }"
             out.append(body[j:m.start()])
@@ -693,6 +734,50 @@ class Lowering:
             j = e + 1
         out.append(body[j:])
         return "".join(out)
+
+    def _check_parent_results(self, f, body, tasks, waits, joins, bare, ln):
+        """--results parent: every result goes to a plain local or parameter,
+        one spawn per local and join, and no return may come between a spawn
+        and the taskwait that joins it (the child writes into this frame)."""
+        for ti, pm in enumerate(tasks):
+            m = CALL.match(body[pm.end():statement_end(body, pm.end())].strip())
+            if not m or not m.group("lhs"):
+                continue
+            if not re.match(r"^[A-Za-z_]\w*$", m.group("lhs").strip()):
+                raise LoweringError("line %d: with --results parent, a task's result must be assigned to a plain "
+                                    "local or parameter, not '%s'" % (ln(pm.start()), m.group("lhs").strip()))
+            w = waits[joins[ti]]
+            if _words(body[pm.end():w.start()], "return"):
+                raise LoweringError("line %d: with --results parent, no return may come between a spawn whose "
+                                    "result is assigned and its taskwait" % ln(pm.start()))
+        for name, sites in bare.items():
+            ks = [joins[ti] for ti, _, _ in sites]
+            if len(ks) != len(set(ks)):
+                raise LoweringError("line %d: with --results parent, '%s' receives two results at one taskwait"
+                                    % (ln(sites[0][1]), name))
+
+    def _parent_function(self, f, readonly, body):
+        """Task text for --results parent: a copy of the frame, loaded from the
+        words the worker read with the header, and the ABI entry point."""
+        return ("__device__ __forceinline__ void %s__gtap_run(void* __frame, int __tid, TaskContext* __ctx, "
+                "const int4& __w0, const int4& __w1, bool __words) {\n"
+                "    %s* __fm = (%s*)__frame;\n"
+                "    %s __fl;\n"
+                "    __gtap_load_frame(&__fl, __fm, __w0, __w1, __words);\n"
+                "    %s* __f = &__fl;\n"
+                "%s"
+                "    int __cc = 0;\n"
+                "    (void)__cc;\n"
+                "    switch (__gtap_get_task_state(__tid)) {\n"
+                "    case 0: {\n%s\n    }\n"
+                "        __gtap_finish_task(__tid, __ctx);\n        return;\n"
+                "    default:\n        __gtap_finish_task(__tid, __ctx);\n        return;\n    }\n}\n"
+                "__device__ void %s(void* __frame, int __tid, TaskContext* __ctx) {\n"
+                "    const int4 __z = make_int4(0, 0, 0, 0);\n"
+                "    %s__gtap_run(__frame, __tid, __ctx, __z, __z, false);\n}\n"
+                % (f.name, f.frame, f.frame, f.frame, f.frame,
+                   "".join("    %s %s = __f->%s;\n    (void)%s;\n" % (p.ctype, p.name, p.name, p.name) for p in readonly),
+                   body, f.task, f.name))
 
     @staticmethod
     def _loop_header(head):
@@ -734,6 +819,8 @@ class Lowering:
         if not lhs:
             # the root task itself is task 0
             fill = "".join("        __e->%s = %s;\n" % (p.name, a) for p, a in zip(g.params, args))
+            if self.parent and g.ret != "void":
+                fill += "        __e->__dst = 0u;\n"
             code = ("if (blockIdx.x == 0 && threadIdx.x == 0) {\n"
                     "        __gtap_push_initial_task(%s, 0);\n"
                     "        %s* __e = (%s*)__gtap_get_task_data(0);\n%s    }\n"
@@ -742,6 +829,8 @@ class Lowering:
         if g.ret == "void":
             raise LoweringError("line %d: '%s' returns nothing" % (line, g.name))
         ef = "__gtap_entry_frame%d" % k
+        if self.parent:
+            return self._parent_entry(g, args, lhs, k, e)
         fields = "".join("    %s a%d;\n" % (p.ctype, i) for i, p in enumerate(g.params)) + "    int __child;\n"
         fill = "".join("        __e->a%d = %s;\n" % (i, a) for i, a in enumerate(args))
         assign = "".join("            __c->%s = __f->a%d;\n" % (p.name, i) for i, p in enumerate(g.params))
@@ -765,6 +854,35 @@ class Lowering:
             "        __gtap_finish_task(__tid, __ctx);\n        return;\n    }\n"
             "    default:\n        __gtap_finish_task(__tid, __ctx);\n        return;\n    }\n}\n"
             % (k, ef, ef, once, g.frame, g.frame, g.task, assign, join, once, lhs, g.frame))
+        code = ("if (blockIdx.x == 0 && threadIdx.x == 0) {\n"
+                "        __gtap_push_initial_task(__gtap_entry%d, 0);\n"
+                "        %s* __e = (%s*)__gtap_get_task_data(0);\n%s    }\n"
+                "    __gtap_execute_task_loop_device();" % (k, ef, ef, fill))
+        return code, e + 1
+
+    def _parent_entry(self, g, args, lhs, k, e):
+        """Entry whose result is assigned, --results parent: the root delivers
+        its result into the entry task's frame."""
+        ef = "__gtap_entry_frame%d" % k
+        fields = "".join("    %s a%d;\n" % (p.ctype, i) for i, p in enumerate(g.params)) + "    %s __res;\n" % g.ret
+        fill = "".join("        __e->a%d = %s;\n" % (i, a) for i, a in enumerate(args))
+        assign = "".join("            __c->%s = __f->a%d;\n" % (p.name, i) for i, p in enumerate(g.params))
+        self.entry_structs.append("struct %s {\n%s};\n"
+                                  "__device__ void __gtap_entry%d(void* __frame, int __tid, TaskContext* __ctx);\n"
+                                  % (ef, fields, k))
+        self.entry_defs.append(
+            "__device__ void __gtap_entry%d(void* __frame, int __tid, TaskContext* __ctx) {\n"
+            "    %s* __f = (%s*)__frame;\n"
+            "    switch (__gtap_get_task_state(__tid)) {\n"
+            "    case 0: {\n        int __cc = 0;\n"
+            "        {\n            %s* __c = (%s*)__gtap_spawn_task(__ctx, __tid, &__cc, %s, 0, nullptr, false);\n"
+            "%s            __c->__dst = __gtap_dst(__tid, offsetof(%s, __res));\n        }\n"
+            "        if (__gtap_set_state_for_join(__tid, __cc, 1, 0)) return;\n    }\n"
+            "    case 1:\n"
+            "        %s = __f->__res;\n"
+            "        __gtap_finish_task(__tid, __ctx);\n        return;\n"
+            "    default:\n        __gtap_finish_task(__tid, __ctx);\n        return;\n    }\n}\n"
+            % (k, ef, ef, g.frame, g.frame, g.task, assign, ef, lhs))
         code = ("if (blockIdx.x == 0 && threadIdx.x == 0) {\n"
                 "        __gtap_push_initial_task(__gtap_entry%d, 0);\n"
                 "        %s* __e = (%s*)__gtap_get_task_data(0);\n%s    }\n"
@@ -804,6 +922,8 @@ class Lowering:
         size_expr = "sizeof(%s)" % sizes[0]
         for s in sizes[1:]:
             size_expr = "(sizeof(%s) > %s ? sizeof(%s) : %s)" % (s, size_expr, s, size_expr)
+        if self.parent:
+            decls += PARENT_HELPERS % size_expr
         # entry tasks, the direct dispatch and the frame size follow the last task function
         tasks = [f.task for f in self.funcs] + ["__gtap_entry%d" % k for k in range(len(self.entry_defs))]
         dispatch = ("__device__ void __gtap_dispatch(unsigned long long __fn, void* __frame, int __tid, "
@@ -812,6 +932,16 @@ class Lowering:
                               % (t, t) for t in tasks)
                     + "    ((void (*)(void*, int, TaskContext*))__fn)(__frame, __tid, __ctx);   // a task not lowered here\n"
                     "}\n")
+        if self.parent:
+            # task functions get the words read with the header; entry tasks read memory
+            dispatch = ("__device__ void __gtap_dispatch_words(unsigned long long __fn, void* __frame, int __tid, "
+                        "TaskContext* __ctx, int4 __w0, int4 __w1) {\n"
+                        + "".join("    if (__fn == (unsigned long long)(void*)&%s) { %s__gtap_run(__frame, __tid, __ctx, "
+                                  "__w0, __w1, true); return; }\n" % (f.task, f.name) for f in self.funcs)
+                        + "".join("    if (__fn == (unsigned long long)(void*)&__gtap_entry%d) { __gtap_entry%d(__frame, "
+                                  "__tid, __ctx); return; }\n" % (k, k) for k in range(len(self.entry_defs)))
+                        + "    ((void (*)(void*, int, TaskContext*))__fn)(__frame, __tid, __ctx);   // a task not lowered here\n"
+                        "}\n")
         tail = ("".join(self.entry_defs) + dispatch
                 + "const size_t __gtap_auto_task_data_size = %s;\n" % size_expr)
         pieces, j = [], 0
@@ -826,17 +956,55 @@ class Lowering:
         pieces.append(src[j:])
         # before any include: the drop-in headers then call the task functions
         # through __gtap_dispatch instead of an indirect call
+        if self.parent:
+            return "#define GTAP_FRAME_WORDS 1\n#include <cstddef>\n#include <cstring>\n" + "".join(pieces)
         return "#define GTAP_DIRECT_DISPATCH 1\n" + "".join(pieces)
 
 
-def lower_source(src, mode=None):
+# --results parent: delivering a child's result into its parent's frame, and
+# a task's copy of its own frame from the words the worker read with the header
+PARENT_HELPERS = """\
+constexpr size_t __gtap_frame_max = %s;
+// frame bytes the worker loads with the task header: 16, or 32 for frames over 16 bytes
+constexpr size_t __gtap_words_bytes = __gtap_frame_max <= 16 ? 16 : 32;
+__device__ __forceinline__ unsigned __gtap_dst(int __tid, size_t __offset) {
+    return (unsigned)__tid * 32u + (unsigned)(__offset / 4) + 1u;
+}
+template <typename T>
+__device__ __forceinline__ void __gtap_deliver(unsigned __dst, T __v) {
+    const unsigned __d = __dst - 1u;
+    *reinterpret_cast<T*>(static_cast<char*>(__gtap_get_task_data((int)(__d >> 5))) + 4u * (__d & 31u)) = __v;
+}
+template <typename F>
+__device__ __forceinline__ void __gtap_load_frame(F* __dst, const F* __mem, const int4& __w0, const int4& __w1,
+                                                  bool __words) {
+    if (!__words) {
+        *__dst = *__mem;
+        return;
+    }
+    constexpr size_t __kw = sizeof(F) < __gtap_words_bytes ? sizeof(F) : __gtap_words_bytes;
+    const int4 __w[2] = {__w0, __w1};
+    memcpy(__dst, __w, __kw);
+    if (sizeof(F) > __kw)
+        memcpy(reinterpret_cast<char*>(__dst) + __kw, reinterpret_cast<const char*>(__mem) + __kw, sizeof(F) - __kw);
+}
+"""
+
+
+def lower_source(src, mode=None, results="retain"):
     """Lowered text of a pragma program; mode 'thread' or 'block' (default:
-    from the gtap header it includes)."""
+    from the gtap header it includes).  results 'retain': a parent reads each
+    child's result from the child's retained frame after the join (the
+    reference's scheme); 'parent' (thread mode): the child writes its result
+    into the parent's frame and tasks read their frames from the words the
+    worker loads with the task header."""
     if mode is None:
         mode = "block" if re.search(r'#\s*include\s*[<"]gtap_block\.cuh[>"]', src) else "thread"
     if mode not in ("thread", "block"):
         raise LoweringError("mode must be 'thread' or 'block'")
-    return Lowering(src, mode).run()
+    if results not in ("retain", "parent"):
+        raise LoweringError("results must be 'retain' or 'parent'")
+    return Lowering(src, mode, results).run()
 
 
 def main(argv=None):
@@ -844,10 +1012,12 @@ def main(argv=None):
     ap.add_argument("input")
     ap.add_argument("-o", "--output", required=True)
     ap.add_argument("--mode", choices=["thread", "block"], default=None)
+    ap.add_argument("--results", choices=["retain", "parent"], default="retain",
+                    help="where a child's result goes: its own retained frame, or the parent's frame")
     a = ap.parse_args(argv)
     try:
         with open(a.input) as f:
-            out = lower_source(f.read(), a.mode)
+            out = lower_source(f.read(), a.mode, a.results)
     except LoweringError as e:
         sys.stderr.write("%s: %s\n" % (a.input, e))
         return 1

@@ -109,6 +109,14 @@ struct TaskContext;
 #ifdef GTAP_DIRECT_DISPATCH
 __device__ void __gtap_dispatch(unsigned long long fn, void* frame, int tid, TaskContext* ctx);
 #endif
+// Programs that define GTAP_FRAME_WORDS (gtap_b200.lower --results parent)
+// provide __gtap_dispatch_words instead: the worker loads the first 16 or 32
+// frame bytes with the task header, in one round trip, and hands them to the
+// task, which then reads its frame from registers.
+#ifdef GTAP_FRAME_WORDS
+__device__ void __gtap_dispatch_words(unsigned long long fn, void* frame, int tid, TaskContext* ctx, int4 w0,
+                                      int4 w1);
+#endif
 
 // Largest task frame in bytes, defined by the lowered program
 // (reference runtime/detail/common/gtap_runtime_common.cuh:9).
@@ -146,16 +154,24 @@ __device__ __forceinline__ gtap::WarpShared& warp_state() {
 
 // Tasks are called through the function pointer __gtap_spawn_task stored.
 struct Program {
+#ifdef GTAP_FRAME_WORDS
+    static constexpr bool kFrameWords = true;
+#else
     static constexpr bool kFrameWords = false;
+#endif
     static constexpr bool kFuncTable = true;
     __device__ static int root_kind(int) { return -1; }   // roots come from __gtap_push_initial_task only
     __device__ static bool root_args_ok(const gtap_root&) { return true; }
     __device__ static void init_root(const gtap::Arena&, const gtap_root&, void*) {}
     __device__ static void warp_leaves(const gtap::Arena&, gtap::WarpShared&, unsigned, int, const int4&,
                                        const int4&) {}
-    __device__ static void exec(const gtap::Arena&, gtap::WarpShared& S, int, int tid, void* frame, const int4&,
-                                const int4&, unsigned long long fn) {
-#ifdef GTAP_DIRECT_DISPATCH
+    __device__ static void exec(const gtap::Arena&, gtap::WarpShared& S, int, int tid, void* frame,
+                                const int4& fw0, const int4& fw1, unsigned long long fn) {
+    (void)fw0;
+    (void)fw1;
+#if defined(GTAP_FRAME_WORDS)
+        __gtap_dispatch_words(fn, frame, tid, reinterpret_cast<TaskContext*>(&S), fw0, fw1);
+#elif defined(GTAP_DIRECT_DISPATCH)
         __gtap_dispatch(fn, frame, tid, reinterpret_cast<TaskContext*>(&S));
 #else
         using Fn = void (*)(void*, int, TaskContext*);

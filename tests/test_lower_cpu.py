@@ -359,3 +359,107 @@ def test_command_line(tmp_path):
     r = subprocess.run([sys.executable, "-m", "gtap_b200.lower", os.path.join(PRAGMA, "fib_pragma.cu"), "-o",
                         str(out), "--mode", "block"], cwd=ROOT, capture_output=True, text=True, timeout=120)
     assert r.returncode == 0 and "__gtap_set_state_for_join_block" in out.read_text()
+
+
+# --results parent (thread mode): children write their results into the
+# parent's frame; tasks read their frames from the words loaded with the header
+def test_parent_results_frame_and_delivery():
+    out = lower_source(read("fib_pragma.cu"), results="parent")
+    assert out.startswith("#define GTAP_FRAME_WORDS 1\n")
+    frame = out[out.index("struct __gtap_frame_fib"):]
+    frame = frame[:frame.index("};")]
+    assert frame.split() == ["struct", "__gtap_frame_fib", "{", "int", "n;", "int", "a;", "int", "b;",
+                             "unsigned", "__dst;"]
+    assert "__c->__dst = __gtap_dst(__tid, offsetof(__gtap_frame_fib, a));" in out
+    assert "__c->__dst = __gtap_dst(__tid, offsetof(__gtap_frame_fib, b));" in out
+    assert "if (__f->__dst) __gtap_deliver<int>(__f->__dst, (__f->a + __f->b));" in out
+    assert "*__fm = *__f; if (__gtap_set_state_for_join(__tid, __cc, 1, 0)) return;" in out
+    assert "__gtap_release_task_id" not in out and "__child" not in out.split("__gtap_entry_frame0")[0]
+    assert "fib__gtap_run(__frame, __tid, __ctx, __w0, __w1, true)" in out
+    assert "__c->__dst = __gtap_dst(__tid, offsetof(__gtap_entry_frame0, __res));" in out
+    assert "d_result = __f->__res;" in out
+
+
+def test_parent_results_root_without_destination():
+    out = lower_source(read("nq_pragma.cu"), results="parent")      # void tasks: no destination field
+    frame = out[out.index("struct __gtap_frame_nq"):]
+    assert "__dst" not in frame[:frame.index("};")]
+    src = read("fib_pragma.cu").replace("    d_result = fib(n);", "    fib(n);")
+    out = lower_source(src, results="parent")
+    assert "__e->__dst = 0u;" in out                                # a root whose result goes nowhere
+
+
+PARENT_BAD = {
+    "block mode": ("tree_block_pragma.cu", None),
+    "result into an array element": (None, """
+#pragma gtap function
+__device__ int f(int n, int* out) {
+    if (n < 2) return n;
+    #pragma gtap task
+    out[0] = f(n - 1, out);
+    #pragma gtap taskwait
+    return out[0];
+}
+"""),
+    "result of another type": (None, """
+#pragma gtap function
+__device__ int f(int n) {
+    if (n < 2) return n;
+    long long a;
+    #pragma gtap task
+    a = f(n - 1);
+    #pragma gtap taskwait
+    return (int)a;
+}
+"""),
+    "two results into one local at one join": (None, """
+#pragma gtap function
+__device__ int f(int n) {
+    if (n < 2) return n;
+    int a;
+    #pragma gtap task
+    a = f(n - 1);
+    #pragma gtap task
+    a = f(n - 2);
+    #pragma gtap taskwait
+    return a;
+}
+"""),
+    "return before the join": (None, """
+#pragma gtap function
+__device__ int f(int n) {
+    if (n < 2) return n;
+    int a;
+    #pragma gtap task
+    a = f(n - 1);
+    if (n == 5) return 0;
+    #pragma gtap taskwait
+    return a;
+}
+"""),
+}
+
+
+@pytest.mark.parametrize("what", sorted(PARENT_BAD))
+def test_parent_results_refusals(what):
+    name, src = PARENT_BAD[what]
+    with pytest.raises(LoweringError):
+        lower_source(read(name) if name else src, results="parent")
+
+
+@pytest.mark.skipif(shutil.which(NVCC) is None, reason="nvcc not available")
+@pytest.mark.parametrize("src,defs", [
+    ("fib_pragma.cu", "-DGTAP_MAX_CHILD_TASKS=2"),
+    ("walk_pragma.cu", ""),
+    ("fib_queues_pragma.cu", "-DGTAP_NUM_QUEUES=3"),
+    ("cilksort_pragma.cu", ""),
+    ("bary_tree_pragma.cu", "-DGTAP_MAX_CHILD_TASKS=8"),
+])
+def test_parent_results_programs_compile(tmp_path, src, defs):
+    low = tmp_path / ("parent_" + src)
+    low.write_text(lower_source(read(src), results="parent"))
+    cmd = [NVCC, "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-diag-suppress", "550",
+           "-I", os.path.join(ROOT, "include"), "-DGTAP_GRID_SIZE=888", "-DGTAP_BLOCK_SIZE=128",
+           "-c", str(low), "-o", str(tmp_path / "prog.o")] + defs.split()
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-3000:]
