@@ -860,6 +860,23 @@ class Lowering:
                 "    __gtap_execute_task_loop_device();" % (k, ef, ef, fill))
         return code, e + 1
 
+    @staticmethod
+    def _bound_kernel(head):
+        """--results parent: give the kernel that holds the entry launch bounds
+        asking for every worker block to be resident (GTAP_GRID_SIZE blocks over
+        148 SMs, at most 32 blocks and 2048 threads per SM), so the compiler
+        keeps the preloaded frame words without raising the register count past
+        what that residency allows."""
+        m = None
+        for m in re.finditer(r"__global__\s+void\s+", head):
+            pass
+        if m is None or "__launch_bounds__" in head[m.start():]:
+            return head
+        per_sm = "((GTAP_GRID_SIZE + 147) / 148)"
+        cap = "(2048 / GTAP_BLOCK_SIZE < 32 ? 2048 / GTAP_BLOCK_SIZE : 32)"
+        bounds = "__launch_bounds__(GTAP_BLOCK_SIZE, (%s < %s ? %s : %s)) " % (per_sm, cap, per_sm, cap)
+        return head[:m.end()] + bounds + head[m.end():]
+
     def _parent_entry(self, g, args, lhs, k, e):
         """Entry whose result is assigned, --results parent: the root delivers
         its result into the entry task's frame."""
@@ -907,7 +924,10 @@ class Lowering:
             if any(f.start <= pm.start() < f.end for f in self.funcs):
                 continue
             code, used = self.lower_entry(src[pm.end():], line_of(src, pm.start()))
-            out.append(src[j:pm.start()])
+            head = src[j:pm.start()]
+            if self.parent:
+                head = self._bound_kernel(head)
+            out.append(head)
             out.append(code)
             j = pm.end() + used
         out.append(src[j:])

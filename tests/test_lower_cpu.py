@@ -2,6 +2,7 @@
 task ABI and the result compiles for sm_100a against the drop-in headers;
 programs outside the supported subset are refused with a LoweringError."""
 import os
+import re
 import shutil
 import subprocess
 
@@ -456,10 +457,20 @@ def test_parent_results_refusals(what):
     ("bary_tree_pragma.cu", "-DGTAP_MAX_CHILD_TASKS=8"),
 ])
 def test_parent_results_programs_compile(tmp_path, src, defs):
+    """Each compiles, and its kernel fits every worker on the GPU at once:
+    888 blocks of 128 threads over 148 SMs is 6 blocks (768 threads) per SM,
+    at most 65536 / 768 = 85 registers a thread; the bounds may spill a few
+    registers."""
     low = tmp_path / ("parent_" + src)
     low.write_text(lower_source(read(src), results="parent"))
     cmd = [NVCC, "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-diag-suppress", "550",
            "-I", os.path.join(ROOT, "include"), "-DGTAP_GRID_SIZE=888", "-DGTAP_BLOCK_SIZE=128",
-           "-c", str(low), "-o", str(tmp_path / "prog.o")] + defs.split()
+           "-Xptxas", "-v", "-c", str(low), "-o", str(tmp_path / "prog.o")] + defs.split()
     r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-3000:]
+    lines = r.stderr.splitlines()
+    k = next(i for i, ln in enumerate(lines) if "Function properties for _Z11exec_kernel" in ln)
+    spilled = int(re.search(r"(\d+) bytes spill stores", lines[k + 1]).group(1))
+    assert spilled <= 64, lines[k + 1]      # a few registers at most (three queues spill 20 bytes)
+    regs = int(re.search(r"Used (\d+) registers", lines[k + 2]).group(1))
+    assert regs <= 85, lines[k + 2]
