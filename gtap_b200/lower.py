@@ -173,7 +173,6 @@ def replace_identifiers(text, names, prefix="__f->"):
 
 
 PRAGMA = re.compile(r"^[ \t]*#[ \t]*pragma[ \t]+gtap[ \t]+(\w+)(.*)$", re.M)
-PRAGMA_AT = re.compile(r"#[ \t]*pragma[ \t]+gtap[ \t]+(\w+)(.*)$", re.M)   # at a known '#' 
 
 
 def parse_queue(rest, line):
