@@ -6,7 +6,7 @@ built from it.  This module lowers the same pragmas, for a restricted subset
 of C++, into the switch state machines the task ABI expects
 (include/gtap_thread.cuh, include/gtap_block.cuh), which nvcc then compiles:
 
-    python -m gtap_b200.lower prog.cu -o prog_lowered.cu [--mode thread|block]
+    python -m gtap_b200.lower prog.cu -o prog_lowered.cu [--mode thread|block] [--results retain|parent]
 
 Pragmas
   #pragma gtap function               before a `__device__ T name(params) {...}`
@@ -49,7 +49,18 @@ Restrictions (reported as LoweringError with the source line):
     uses; no local shadows a parameter;
   * a spawn whose result is assigned is not inside a loop, and the next
     taskwait after it is in its own block or an enclosing one;
-  * task functions are only called through `#pragma gtap task` / `entry`.
+  * task functions are only called through `#pragma gtap task` / `entry`;
+  * a result is assigned with `=`, not a compound assignment.
+
+--results parent (thread mode, experimental): instead of retained child
+frames, a child with a result writes it into its parent's frame (through a
+4-byte destination word in its own frame) before it finishes, and every task
+reads its frame from the words the worker loads with the task header
+(GTAP_FRAME_WORDS, __gtap_dispatch_words), working on a copy that is written
+back before a join.  Results then go to plain locals or parameters of the
+callee's return type, one per local and join, with no return between a spawn
+and its join; the entry kernel gets launch bounds that keep every worker
+resident.
 """
 import argparse
 import re
