@@ -76,4 +76,6 @@ inline unsigned long long atomicAdd(unsigned long long* p, unsigned long long v)
 }
 inline long long __double_as_longlong(double d) { long long r; memcpy(&r, &d, sizeof(r)); return r; }
 inline int __ffsll(long long x) { return __builtin_ffsll(x); }
+inline int __ffs(int x) { return __builtin_ffs(x); }
+inline void __threadfence() {}
 inline void __syncthreads() {}

@@ -141,3 +141,27 @@ def test_emulator_catches_a_missing_write_back(emu_bins, tmp_path):
     assert r.returncode == 0, r.stderr[-2000:]
     out = run(str(exe), "lifo", 1, 6, 0)
     assert out["result"] != walk_expect(6, 0)
+
+
+@pytest.mark.parametrize("order,seed", ORDERS)
+def test_hand_lowered_programs(tmp_path, order, seed):
+    """The hand-lowered reference programs (tests/lowered) follow the same
+    protocol under the emulator (the cilksort one holds inline PTX loads and
+    runs on the GPU only)."""
+    if shutil.which(CXX) is None:
+        pytest.skip("no host C++ compiler")
+    for name, defs, args, check in [
+        ("fib_lowered", "", (22, 0, 1), lambda r: r["result"] == orc.fib(22)),
+        ("fib_lowered", "", (24, 10, 1), lambda r: r["result"] == orc.fib(24)),
+        ("nq_lowered", "-DGTAP_ASSUME_NO_TASKWAIT", (9, 4, 1), lambda r: r["result"] == orc.nq(9)),
+    ]:
+        with open(os.path.join(ROOT, "tests", "lowered", name + ".cu")) as f:
+            text = re.sub(r"(\w+)<<<[^>]*>>>\(", r"\1(", f.read())
+        cu = tmp_path / (name + ".cpp")
+        cu.write_text(text)
+        exe = tmp_path / name
+        r = subprocess.run([CXX, "-std=c++17", "-O1", "-w", "-I", EMU, str(cu), "-o", str(exe)] + defs.split(),
+                           capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr[-2000:]
+        out = run(str(exe), order, seed, *args)
+        assert out["error_code"] == 0 and check(out), out
