@@ -6,6 +6,7 @@
 // rewrites `k<<<g, b>>>(...)` to `k(...)`); atomics are plain updates (the
 // emulator runs one task at a time).
 #pragma once
+#include <climits>
 #include <cmath>
 #include <cstddef>
 #include <cstdint>
@@ -17,6 +18,7 @@
 #define __device__
 #define __host__
 #define __shared__ static
+#define __constant__
 #define __forceinline__ inline
 #define __noinline__
 #define __restrict__ __restrict

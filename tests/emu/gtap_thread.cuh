@@ -46,6 +46,23 @@ void __gtap_dispatch(unsigned long long fn, void* frame, int tid, TaskContext* c
 void __gtap_dispatch_words(unsigned long long fn, void* frame, int tid, TaskContext* ctx, int4 w0, int4 w1);
 #endif
 
+// the device helpers the drop-in header gives task code (include/gtap_device_util.cuh)
+inline int load_L2(int* p) { return *p; }
+inline unsigned load_L2(unsigned* p) { return *p; }
+inline uint16_t load_L2_u16t(uint16_t* p) { return *p; }
+inline int load_L2_acquire(int* p) { return *p; }
+inline void store_L2(int* p, int v) { *p = v; }
+inline void store_L2(unsigned* p, unsigned v) { *p = v; }
+inline void store_L2_release(int* p, int v) { *p = v; }
+inline int atomicCAS_acquire(int* p, int expected, int desired) {
+    const int old = *p;
+    if (old == expected) *p = desired;
+    return old;
+}
+inline unsigned get_lane_id() { return 0; }
+inline unsigned get_warp_id_in_block() { return 0; }
+inline unsigned get_warp_id_global() { return 0; }
+
 namespace gtap_emu {
 
 constexpr size_t kFrameBytes = 256;
