@@ -77,7 +77,8 @@ struct Rec {
 
 struct Emu {
     std::deque<Rec> recs;   // records never move while a task holds a frame pointer
-    std::vector<int> free_ids, ready, staged;
+    std::vector<int> free_ids, staged;
+    std::deque<int> ready;
     std::mt19937_64 rng{1};
     int order = 0;   // 0 lifo, 1 fifo, 2 random
     int error = 0;
@@ -257,9 +258,19 @@ inline void __gtap_execute_task_loop_device() {
     using namespace gtap_emu;
     Emu& E = emu();
     while (!E.ready.empty() && !E.error) {
-        size_t i = E.order == 0 ? E.ready.size() - 1 : E.order == 1 ? 0 : (size_t)(E.rng() % E.ready.size());
-        const int tid = E.ready[i];
-        E.ready.erase(E.ready.begin() + (long)i);
+        int tid;
+        if (E.order == 0) {
+            tid = E.ready.back();
+            E.ready.pop_back();
+        } else if (E.order == 1) {
+            tid = E.ready.front();
+            E.ready.pop_front();
+        } else {
+            const size_t i = (size_t)(E.rng() % E.ready.size());
+            tid = E.ready[i];
+            E.ready[i] = E.ready.back();   // any order among the rest: the next pick is random too
+            E.ready.pop_back();
+        }
         run_one(tid);
     }
     for (size_t i = 0; i < E.recs.size() && !E.error; ++i)
