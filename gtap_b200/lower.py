@@ -926,15 +926,27 @@ class Lowering:
             fr, fn = self.lower_function(f)
             frames.append(fr)
             bodies.append(fn)
-        # entries, outside the task functions
+        # entries, outside the task functions.  An entry task (an entry whose
+        # result is assigned) goes right before the kernel that holds the
+        # entry, where everything that kernel uses is declared; when the
+        # kernel comes before the task functions it goes after the last one.
         out, j = [], 0
+        last_task_end = max(f.end for f in self.funcs)
+        tail_defs = []
         for pm in PRAGMA.finditer(src):
             if pm.group(1) != "entry":
                 continue
             if any(f.start <= pm.start() < f.end for f in self.funcs):
                 continue
+            n_defs = len(self.entry_defs)
             code, used = self.lower_entry(src[pm.end():], line_of(src, pm.start()))
             head = src[j:pm.start()]
+            new_defs = "".join(self.entry_defs[n_defs:])
+            g = head.rfind("__global__")
+            if new_defs and g >= 0 and j + g >= last_task_end:
+                head = head[:g] + new_defs + head[g:]
+            else:
+                tail_defs.append(new_defs)
             if self.parent:
                 head = self._bound_kernel(head)
             out.append(head)
@@ -972,7 +984,7 @@ class Lowering:
                                   "__tid, __ctx); return; }\n" % (k, k) for k in range(len(self.entry_defs)))
                         + "    ((void (*)(void*, int, TaskContext*))__fn)(__frame, __tid, __ctx);   // a task not lowered here\n"
                         "}\n")
-        tail = ("".join(self.entry_defs) + dispatch
+        tail = ("".join(tail_defs) + dispatch
                 + "const size_t __gtap_auto_task_data_size = %s;\n" % size_expr)
         pieces, j = [], 0
         for k, f in enumerate(funcs):

@@ -165,3 +165,51 @@ def test_hand_lowered_programs(tmp_path, order, seed):
         assert r.returncode == 0, r.stderr[-2000:]
         out = run(str(exe), order, seed, *args)
         assert out["error_code"] == 0 and check(out), out
+
+
+EDGE_MAIN = r"""
+__device__ int d_result;
+
+__global__ void exec_kernel(int n) {
+    #pragma gtap entry
+    d_result = f(n);
+}
+
+int main(int argc, char** argv) {
+    const int n = atoi(argv[1]);
+    gtap_initialize();
+    exec_kernel<<<GTAP_GRID_SIZE, GTAP_BLOCK_SIZE>>>(n);
+    gtap_synchronize();
+    int result = -1, code = 0;
+    cudaMemcpyFromSymbol(&result, d_result, sizeof(int));
+    gtap_get_runtime_error_code(&code);
+    printf("{\"result\": %d, \"error_code\": %d}\n", result, code);
+    return code != 0;
+}
+"""
+
+
+@pytest.mark.parametrize("results", ["retain", "parent"])
+@pytest.mark.parametrize("name,expect", [
+    ("comments_strings", lambda n: orc.fib(n)),      # fib with comments and strings holding braces
+    ("else_if", lambda n: orc.fib(n)),               # fib through an else-if chain, a taskwait per branch
+    ("decl_init", lambda n: 0 if n == 0 else 1),     # f(n) = f(n - 1), from a spawn-initialised local
+])
+def test_edge_programs_run(tmp_path, results, name, expect):
+    if shutil.which(CXX) is None:
+        pytest.skip("no host C++ compiler")
+    from tests.test_lower_cpu import EDGE
+    if results == "parent" and name == "decl_init":
+        pytest.skip("a declaration initialised by a spawn is a retained-frame form")
+    text = lower_source(EDGE[name] + EDGE_MAIN, mode="thread", results=results)
+    text = re.sub(r"(\w+)<<<[^>]*>>>\(", r"\1(", text)
+    cu = tmp_path / (name + ".cpp")
+    cu.write_text("#include <cstdlib>\n" + text)
+    exe = tmp_path / name
+    r = subprocess.run([CXX, "-std=c++17", "-O1", "-w", "-I", EMU, str(cu), "-o", str(exe)],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    for order, seed in ORDERS:
+        for n in (0, 1, 2, 11):
+            out = run(str(exe), order, seed, n)
+            assert out["error_code"] == 0 and out["result"] == expect(n), (order, n, out)
