@@ -2,9 +2,10 @@
 // runtime calls, qualifiers and intrinsics that the pragma programs in
 // tests/pragma use, so that their lowered text compiles with g++ and runs
 // on the CPU under the task-ABI emulator in gtap_thread.cuh (this folder).
-// Device memory is host memory; a kernel launch is a plain call (the test
-// rewrites `k<<<g, b>>>(...)` to `k(...)`); atomics are plain updates (the
-// emulator runs one task at a time).
+// Device memory is host memory; a kernel launch runs the kernel body as one
+// block (the test rewrites `k<<<g, b>>>(args)` to `emu_launch([&] { k(args); })`):
+// one thread in thread mode, a pool of threads in block mode, whose
+// __syncthreads is a barrier; atomics are host atomics.
 #pragma once
 #include <climits>
 #include <cmath>
@@ -13,6 +14,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <thread>
+#include <vector>
 
 #define __global__
 #define __device__
@@ -27,7 +30,37 @@
 struct emu_dim3 {
     unsigned x, y, z;
 };
-static emu_dim3 threadIdx = {0, 0, 0}, blockIdx = {0, 0, 0}, blockDim = {1, 1, 1}, gridDim = {1, 1, 1};
+static thread_local emu_dim3 threadIdx = {0, 0, 0};
+static emu_dim3 blockIdx = {0, 0, 0}, blockDim = {1, 1, 1}, gridDim = {1, 1, 1};
+
+// threads that run each emulated block (1 in thread mode; the block-mode
+// emulator sets it), and the barrier __syncthreads calls (none with one thread)
+inline int& emu_block_threads() {
+    static int t = 1;
+    return t;
+}
+inline void (*&emu_sync_hook())() {
+    static void (*h)() = nullptr;
+    return h;
+}
+// a kernel launch: the kernel body on emu_block_threads() threads of one block
+template <class F>
+inline void emu_launch(F f) {
+    const int T = emu_block_threads();
+    blockDim.x = (unsigned)T;
+    if (T == 1) {
+        threadIdx.x = 0;
+        f();
+        return;
+    }
+    std::vector<std::thread> ts;
+    for (int i = 0; i < T; ++i)
+        ts.emplace_back([&f, i] {
+            threadIdx.x = (unsigned)i;
+            f();
+        });
+    for (auto& t : ts) t.join();
+}
 
 struct int4 {
     int x, y, z, w;
@@ -69,15 +102,25 @@ inline cudaError_t cudaDeviceSynchronize() { return cudaSuccess; }
 inline cudaError_t cudaSetDevice(int) { return cudaSuccess; }
 inline const char* cudaGetErrorString(cudaError_t) { return "emulated"; }
 
-inline int atomicAdd(int* p, int v) { int o = *p; *p += v; return o; }
-inline unsigned atomicAdd(unsigned* p, unsigned v) { unsigned o = *p; *p += v; return o; }
+inline int atomicAdd(int* p, int v) { return __atomic_fetch_add(p, v, __ATOMIC_SEQ_CST); }
+inline unsigned atomicAdd(unsigned* p, unsigned v) { return __atomic_fetch_add(p, v, __ATOMIC_SEQ_CST); }
 inline unsigned long long atomicAdd(unsigned long long* p, unsigned long long v) {
-    unsigned long long o = *p;
-    *p += v;
+    return __atomic_fetch_add(p, v, __ATOMIC_SEQ_CST);
+}
+inline int atomicMin(int* p, int v) {
+    int o = __atomic_load_n(p, __ATOMIC_SEQ_CST);
+    while (v < o && !__atomic_compare_exchange_n(p, &o, v, false, __ATOMIC_SEQ_CST, __ATOMIC_SEQ_CST)) {
+    }
     return o;
+}
+inline int atomicCAS(int* p, int expected, int desired) {
+    __atomic_compare_exchange_n(p, &expected, desired, false, __ATOMIC_SEQ_CST, __ATOMIC_SEQ_CST);
+    return expected;
 }
 inline long long __double_as_longlong(double d) { long long r; memcpy(&r, &d, sizeof(r)); return r; }
 inline int __ffsll(long long x) { return __builtin_ffsll(x); }
 inline int __ffs(int x) { return __builtin_ffs(x); }
 inline void __threadfence() {}
-inline void __syncthreads() {}
+inline void __syncthreads() {
+    if (emu_sync_hook()) emu_sync_hook()();
+}

@@ -217,3 +217,45 @@ def test_edge_programs_run(tmp_path, results, name, expect):
         for n in (0, 1, 2, 11):
             out = run(str(exe), order, seed, n)
             assert out["error_code"] == 0 and out["result"] == expect(n), (order, n, out)
+
+
+def build_block(tmp_path, name, text, defs=""):
+    """A block-mode program for the block emulator (tests/emu/gtap_block.cuh):
+    launches run on a block of 32 host threads."""
+    text = re.sub(r"(\w+)<<<[^>]*>>>\((.*)\);", r"emu_launch([&] { \1(\2); });", text)
+    cu = tmp_path / (name + ".cpp")
+    cu.write_text(text)
+    exe = tmp_path / name
+    r = subprocess.run([CXX, "-std=c++17", "-O1", "-w", "-pthread", "-I", EMU, "-DGTAP_BLOCK_SIZE=32", str(cu),
+                        "-o", str(exe)] + defs.split(), capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    return str(exe)
+
+
+@pytest.fixture(scope="module")
+def block_bins(tmp_path_factory):
+    if shutil.which(CXX) is None:
+        pytest.skip("no host C++ compiler")
+    d = tmp_path_factory.mktemp("emu_block")
+    bins = {}
+    for name in ("tree_block_pragma", "bary_block_pragma"):
+        with open(os.path.join(PRAGMA, name + ".cu")) as f:
+            bins[name] = build_block(d, name, lower_source(f.read()))
+    with open(os.path.join(ROOT, "tests", "lowered", "tree_block_lowered.cu")) as f:
+        bins["tree_block_lowered"] = build_block(d, "tree_block_lowered", f.read())
+    return bins
+
+
+@pytest.mark.parametrize("order,seed", ORDERS)
+def test_block_mode_programs(block_bins, order, seed):
+    from tests.test_gpu_dropin_block import tree_expect
+    for height, work in [(0, 10), (3, 100), (7, 300)]:
+        r = run(block_bins["tree_block_pragma"], order, seed, height, work)
+        assert r["error_code"] == 0 and r["result"] == tree_expect(height, work)
+        r = run(block_bins["tree_block_lowered"], order, seed, height, work, 1)
+        assert r["error_code"] == 0 and r["result"] == tree_expect(height, work)
+    for D, B, mem_ops, iters, log2n in [(0, 3, 4, 4, 8), (5, 3, 64, 256, 10), (8, 4, 40, 70, 12)]:
+        s = 5 + D
+        r = run(block_bins["bary_block_pragma"], order, seed, D, B, mem_ops, iters, log2n, s, 1)
+        assert r["error_code"] == 0 and r["threads"] == 32
+        assert (r["sum"], r["nodes"]) == orc.bary_tree_block(D, B, mem_ops, iters, 32, orc.bary_input(s, 1 << log2n))
