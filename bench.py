@@ -10,7 +10,10 @@ starts; the key slabs (~2.6 GB) exceed L2, and each step's cilksort leaves
 read the pristine input, so no restore happens between steps.
 
 Prints ONE JSON line (rank 0).  --impl reference times the reference's
-sequential programs (CPU) on a bounded sample of the same roots.
+sequential programs (CPU, the oracle's restatement of seq_fib.c / seq_nq.c /
+seq_cilksort.cpp) on a bounded sample of the same roots; it builds the mix
+with the oracle's own generators and never loads libgtap_b200.so.  Both arms
+print the same `config` object.
 """
 import argparse
 import ctypes
@@ -27,6 +30,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+# plain-Python modules of the package: importing them loads no library
 from gtap_b200.workloads import MERGE_CUTOFF, MIX_SEED, N_ROOTS, SORT_CUTOFF, Mix  # noqa: E402
 from gtap_b200.autotune import load_tuned  # noqa: E402
 
@@ -58,6 +62,8 @@ def parse():
                     help="roots per serve session (BFS on R-MAT 16-20 / tree sums 2^18-2^20); 0 = no serve run")
     ap.add_argument("--config", default="", help="json dict of gtap_config overrides (applied last)")
     ap.add_argument("--tuned", default=TUNED, help="autotuner result whose overrides are applied first ('' = none)")
+    ap.add_argument("--no-reference-gpu", dest="reference_gpu", action="store_false",
+                    help="skip the fib comparison with the reference GTaP GPU build")
     return ap.parse_args()
 
 
@@ -149,68 +155,106 @@ class Clocks:
 # ---------------------------------------------------------------------------
 # CPU baseline: the reference's sequential recursions on a bounded sample
 # ---------------------------------------------------------------------------
-def _cpu_worker(job):
-    kind, param, seed = job
-    sys.path.insert(0, ROOT)
-    from tests import oracle_lib as orc
-    L = orc.load()
-    if kind == 2:
-        keys = orc.keys(int(seed) & 0xFFFFFFFF, int(param))
-        tmp = np.empty_like(keys)
-        t0 = time.perf_counter()
-        L.orc_seq_cilksort(orc.p(keys), orc.p(tmp), len(keys))
-        dt = time.perf_counter() - t0
-        assert np.all(keys[1:] >= keys[:-1])
-        return dt
-    t0 = time.perf_counter()
-    L.orc_seq_root(int(kind), int(param), int(seed))
-    return time.perf_counter() - t0
+class OracleGenerators:
+    """The oracle's restatement of the seeded generators (std::mt19937_64 root
+    mix, std::mt19937 keys).  The reference arm builds the mix with these, so
+    it never loads the product library."""
+
+    def __init__(self):
+        from tests import oracle_lib as orc
+        self.orc = orc
+
+    def gen_mix(self, seed, n):
+        return self.orc.root_mix(seed, n)
+
+    def gen_keys(self, seed, n):
+        return self.orc.keys(seed, n)
 
 
-def cpu_baseline(mix, tasks_of, target_s, cores):
-    """Sample roots (seeded order) until the summed single-core time estimate
-    reaches target_s * cores; run them on `cores` processes; report tasks/s.
-    tasks_of(i) gives root i's task count in the GPU formulation."""
-    import multiprocessing as mp
-    # cost model only decides the sample size; the timing below is measured
+def workload_config(mix):
+    """The `config` object both arms print (identical by construction)."""
+    return {"workload": "batched 4096-root mix: fib(n in [18,28], cutoff 0), n-queens(n in [8,11], one task per "
+                        "row), cilksort of 2^10..2^20 std::mt19937 int32 keys (cutoffs 64/256)",
+            "roots": int(mix.n), "mix_seed": MIX_SEED, "cilksort_keys": int(mix.total_keys),
+            "l2": "inputs larger than L2 (%.2f GB of key slabs: source, output, scratch)"
+                  % (3 * mix.total_keys * 4 / 1e9)}
+
+
+def cpu_sample(mix, target_s, cores):
+    """Roots (seeded order) whose summed single-core time estimate reaches
+    target_s * cores.  The cost model only sizes the sample."""
     nq_nodes = {8: 2057, 9: 8394, 10: 35539, 11: 166926}   # search-tree nodes of n-queens(n)
     est = {0: lambda p: 1.6e-9 * 1.618 ** p, 1: lambda p: 1.2e-8 * nq_nodes.get(p, 6.0 ** p),
            2: lambda p: 9e-8 * p}
     budget = target_s * cores
     order = np.random.RandomState(7).permutation(mix.n)
-    jobs, tasks, spent = [], 0, 0.0
+    picked, spent = [], 0.0
     for i in order:
-        k, p = int(mix.kind[i]), int(mix.param[i])
-        c = est[k](p)
-        if spent + c > budget and jobs:
+        c = est[int(mix.kind[i])](int(mix.param[i]))
+        if spent + c > budget and picked:
             continue
-        jobs.append((k, p, int(mix.seed[i])))
-        tasks += int(tasks_of(int(i)))
+        picked.append(int(i))
         spent += c
         if spent >= budget:
             break
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(cores) as pool:
-        pool.map(_cpu_worker, [(0, 2, 0)] * cores)   # warm the workers
-        t0 = time.perf_counter()
-        pool.map(_cpu_worker, jobs, chunksize=1)
-        wall = time.perf_counter() - t0
-    return {"value": tasks / wall, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": "%d of %d mix roots (seq_fib.c / seq_nq.c / seq_cilksort.cpp recursions, -O2), %.1f s wall"
-                      % (len(jobs), mix.n, wall),
-            "wall_s": wall, "tasks": tasks}
+    return picked
 
 
-def mix_tasks_oracle(mix):
-    """Per-root task counts for the CPU sample (fib/nq exact, cilksort by recursion)."""
+def cpu_baseline(mix, sample, tasks_of, cores, steps=1):
+    """The sample's roots on `cores` host threads (each a C call that releases
+    the GIL): fib / n-queens as the sequential recursions of seq_fib.c /
+    seq_nq.c, cilksort as seq_cilksort.cpp's recursion on a fresh copy of the
+    root's keys.  Keys are copied before the timed region; each step's wall
+    time covers only the recursions.  Returns one tasks/s figure per step."""
+    from concurrent.futures import ThreadPoolExecutor
     from tests import oracle_lib as orc
-    out = np.zeros(mix.n, np.int64)
-    for i in range(mix.n):
+    L = orc.load()
+    tasks = int(sum(int(tasks_of(i)) for i in sample))
+    # largest jobs first: the makespan is not set by a big root started last
+    sample = sorted(sample, key=lambda i: -(int(mix.param[i]) * (50 if mix.kind[i] == 2 else 1)))
+    values, walls = [], []
+    with ThreadPoolExecutor(cores) as pool:
+        for _ in range(steps):
+            bufs = {}
+            for i in sample:
+                if int(mix.kind[i]) == 2:
+                    o, n = int(mix.offsets[i]), int(mix.param[i])
+                    bufs[i] = (mix.keys[o:o + n].copy(), np.empty(n, np.int32))
+
+            def job(i):
+                k = int(mix.kind[i])
+                if k == 2:
+                    a, t = bufs[i]
+                    L.orc_seq_cilksort(orc.p(a), orc.p(t), len(a))
+                else:
+                    L.orc_seq_root(k, int(mix.param[i]), int(mix.seed[i]))
+
+            t0 = time.perf_counter()
+            list(pool.map(job, sample))
+            wall = time.perf_counter() - t0
+            for a, _ in bufs.values():
+                assert np.all(a[1:] >= a[:-1])
+            values.append(tasks / wall)
+            walls.append(wall)
+    return values, walls, tasks
+
+
+def mix_tasks_oracle(mix, sample):
+    """Per-root task counts of the sampled roots: fib / n-queens from the
+    recursions' closed counts, cilksort by running the oracle's cilksort
+    recursion on the root's keys (its merge splits depend on them)."""
+    from tests import oracle_lib as orc
+    out = {}
+    for i in sample:
         k, p = int(mix.kind[i]), int(mix.param[i])
         if k == 0:
             out[i] = orc.fib_tasks(p, 0)
         elif k == 1:
             out[i] = orc.nq_tasks(p, p - 1)
+        else:
+            o = int(mix.offsets[i])
+            _, st, mt = orc.cilksort(mix.keys[o:o + p], SORT_CUTOFF, MERGE_CUTOFF)
+            out[i] = st + mt
     return out
 
 
@@ -218,35 +262,21 @@ def mix_tasks_oracle(mix):
 def run_reference(args, rank):
     if rank != 0:
         return
-    import gtap_b200 as gt
-    from tests import oracle_lib as orc
-    mix = Mix(gt, args.roots)
-    tpr = mix_tasks_oracle(mix)
-
-    def tasks_of(i):
-        if int(mix.kind[i]) == 2 and tpr[i] == 0:
-            # the cilksort task tree depends on the keys (merge splits): count it
-            # with the oracle recursion on this root's keys
-            n = int(mix.param[i])
-            o = int(mix.offsets[i])
-            _, st, mt = orc.cilksort(mix.keys[o:o + n], SORT_CUTOFF, MERGE_CUTOFF)
-            tpr[i] = st + mt
-        return tpr[i]
-
+    mix = Mix(OracleGenerators(), args.roots)
     cores = os.cpu_count() or 1
-    per_step = []
-    cb = None
-    for s in range(args.warmup + args.steps):
-        cb = cpu_baseline(mix, tasks_of, max(2.0, args.cpu_sample_s / max(1, args.steps)), cores)
-        if s >= args.warmup:
-            per_step.append(cb["value"])
-    v = statistics.median(per_step)
+    sample = cpu_sample(mix, max(2.0, args.cpu_sample_s / max(1, args.steps)), cores)
+    tpr = mix_tasks_oracle(mix, sample)
+    _, _, _ = cpu_baseline(mix, sample, tpr.get, cores, steps=max(1, args.warmup))   # warm-up steps
+    values, walls, tasks = cpu_baseline(mix, sample, tpr.get, cores, steps=args.steps)
+    v = statistics.median(values)
+    cb = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+          "sample": "%d of %d mix roots per step (%d tasks): the oracle's restatement of seq_fib.c / seq_nq.c / "
+                    "seq_cilksort.cpp, -O2, one root per host thread" % (len(sample), mix.n, tasks)}
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded mix, mt19937 keys)",
-            "config": {"workload": "batched 4096-root mix (fib 18-28 / nq 8-11 / cilksort 2^10-2^20)",
-                       "roots": args.roots, "mix_seed": MIX_SEED},
-            "cpu_baseline": {**cb, "value": v},
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.median(walls) * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic (seeded mix, mt19937 keys)", "config": workload_config(mix),
+            "cpu_baseline": cb,
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -276,11 +306,12 @@ def main():
     tmp = torch.empty_like(src)
     roots = mix.roots(gt, src.data_ptr(), arr.data_ptr(), tmp.data_ptr())
 
-    # warm-up (also verifies results)
-    res = None
-    for _ in range(args.warmup):
+    # warm-up (the first launch's results are verified)
+    res, verified = None, False
+    for w in range(max(1, args.warmup)):
         res, st = gt.launch(roots)
-    verified = verify(gt, mix, res, src, arr)
+        if w == 0:
+            verified = verify(gt, mix, res, src, arr)
 
     clocks = Clocks(torch.cuda.current_device())
     clocks.start()
@@ -289,7 +320,7 @@ def main():
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    kern_ms, tasks_step, execs_step, stats_acc = [], [], [], None
+    kern_ms, tasks_step, stats_acc = [], [], None
     e0.record()
     for _ in range(args.steps):
         res, st = gt.launch(roots)
@@ -304,6 +335,8 @@ def main():
     ms_max = max_over_ranks(e0.elapsed_time(e1), world, "cuda")
     tasks_per_step = int(statistics.median(tasks_step))
     value = world * tasks_per_step * args.steps / (ms_max / 1e3)
+    # the last timed launch's results must be the verified ones
+    verified = verified and all(r.status == gt.ROOT_DONE for r in res) and tasks_per_step == tasks_step[0]
 
     # roofline: dominant kernel = the persistent worker
     alg_bytes = algorithmic_bytes(mix, res)
@@ -317,10 +350,12 @@ def main():
     peak_src = "measured" if hbm else "fallback"
     hbm = hbm or 6650.0
     achieved = alg_bytes / (k_ms / 1e3) / 1e9
+    counters = stats_acc.as_dict() if stats_acc else {}
     roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
             "traffic": traffic_from_profile(), "peak_source": peak_src,
             "kernel": "gtap::thread_worker_kernel<BuiltinProgram>", "kernel_ms": k_ms,
-            "algorithmic_bytes_per_launch": alg_bytes}
+            "algorithmic_bytes_per_launch": alg_bytes,
+            "atomic": atomic_view(counters, mix, res, k_ms)}
 
     # e2e through the host-buffer entry point (H2D keys, D2H sorted keys + results)
     e2e = None
@@ -328,21 +363,11 @@ def main():
         e2e = measure_e2e(gt, mix, args.steps, tasks_per_step, world, arr)
 
     # per-root launch baseline (gtap_reset-style relaunch per root), 1 step,
-    # with the library's default configuration (the batch-tuned one favours
-    # many roots in flight, not one)
+    # under its own best configuration among the library defaults and the
+    # batch-tuned one
     per_root = None
     if not args.no_per_root:
-        gt.gtap_finalize()
-        gt.gtap_initialize(gt.default_config())
-        torch.cuda.synchronize()
-        p0 = time.perf_counter()
-        res_pr, st_pr = gt.launch(roots, per_root=True)
-        torch.cuda.synchronize()
-        pr_s = time.perf_counter() - p0
-        ok_pr = all(a.value == b.value and a.status == b.status for a, b in zip(res_pr, res))
-        per_root = {"tasks_per_s": sum(r.tasks for r in res_pr) / pr_s, "s_per_step": pr_s,
-                    "kernel_ms_sum": st_pr.kernel_ms, "results_match": ok_pr, "config": "library defaults",
-                    "speedup_batched_vs_per_root": value / world / (sum(r.tasks for r in res_pr) / pr_s)}
+        per_root = measure_per_root(gt, roots, res, value / world, overrides)
 
     # serve mode: capacity, then Poisson arrivals at fractions of it and at
     # 2000 roots/s (the lowest served rate asked for), library defaults
@@ -376,29 +401,40 @@ def main():
         msort = measure_mergesort_thread(gt, args.mergesort_keys, args.steps, args.warmup, hbm_peak=hbm,
                                          overrides=json.loads(args.config) if args.config else {})
 
+    # the reference GTaP GPU build on fib, beside this runtime (same box, same call)
+    ref_gpu = None
+    if args.reference_gpu and rank == 0:
+        gt.gtap_finalize()
+        ref_gpu = measure_reference_gpu(gt)
+
     cpu = None
     if not args.no_cpu and rank == 0 and world == 1:
         tasks_gpu = [r.tasks for r in res]
-        cpu = cpu_baseline(mix, lambda i: tasks_gpu[i], args.cpu_sample_s, os.cpu_count() or 1)
+        cores = os.cpu_count() or 1
+        sample = cpu_sample(mix, args.cpu_sample_s, cores)
+        vals, walls, ntasks = cpu_baseline(mix, sample, lambda i: tasks_gpu[i], cores)
+        cpu = {"value": vals[0], "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": "%d of %d mix roots (%d tasks), %.1f s wall: the oracle's restatement of seq_fib.c / "
+                         "seq_nq.c / seq_cilksort.cpp, -O2, one root per host thread"
+                         % (len(sample), mix.n, ntasks, walls[0])}
 
-    counters = stats_acc.as_dict() if stats_acc else {}
+    W = int(counters.get("workers", 0))
+    sched = {"steal_success_rate": counters.get("steal_successes", 0) / max(1, counters.get("steal_attempts", 0)),
+             "idle_worker_fraction": counters.get("idle_ns", 0) / max(1.0, W * kern_ms[-1] * 1e6),
+             "workers": W, "idle_polls": counters.get("idle_polls", 0),
+             "executions": counters.get("executions", 0), "rounds": counters.get("rounds", 0),
+             "tasks_per_round": counters.get("executions", 0) / max(1, counters.get("rounds", 0))}
+    # order: the contract's keys first, the large per-mode objects next, the
+    # short summaries last (they stay in view when the line is cut short)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded mix, mt19937 keys)",
-            "config": {"workload": "batched 4096-root mix (fib 18-28 / nq 8-11 one task per row / "
-                                   "cilksort 2^10-2^20, cutoffs 64/256)",
-                       "roots": args.roots, "mix_seed": MIX_SEED, "tasks_per_step": tasks_per_step,
-                       "l2": "inputs larger than L2 (%.2f GB key slabs)" % (3 * mix.total_keys * 4 / 1e9),
-                       "parallelism": "replicas" if world > 1 else "single GPU",
-                       "runtime": {k: v for k, v in cfg.as_dict().items()}, "tuned_from": tuned_from},
+            "config": workload_config(mix), "tasks_per_step": tasks_per_step,
+            "parallelism": "replicas" if world > 1 else "single GPU",
+            "runtime": {"config": cfg.as_dict(), "tuned_from": tuned_from},
             "verified": verified, "gpu_launches": 2 * args.steps, "e2e": e2e, "roofline": roof,
-            "cpu_baseline": cpu, "per_root_launch": per_root, "serve": serve, "block_mode": block, "mergesort_thread": msort,
-            "clocks": ck,
-            "scheduler": {"steal_success_rate": counters.get("steal_successes", 0) /
-                          max(1, counters.get("steal_attempts", 0)),
-                          "idle_polls": counters.get("idle_polls", 0),
-                          "executions": counters.get("executions", 0), "rounds": counters.get("rounds", 0),
-                          "tasks_per_round": counters.get("executions", 0) / max(1, counters.get("rounds", 0))}}
+            "cpu_baseline": cpu, "clocks": ck, "serve": serve, "block_mode": block, "mergesort_thread": msort,
+            "reference_gpu": ref_gpu, "per_root_launch": per_root, "scheduler": sched}
     if rank == 0:
         print(json.dumps(line), flush=True)
     gt.gtap_finalize()
@@ -518,6 +554,12 @@ def measure_block_cilksort(gt, n, steps, warmup, cpu, hbm_peak, overrides=None):
 
 
 def verify(gt, mix, res, src, arr):
+    """Every root of the mix against the oracle, exactly: fib and n-queens
+    values and task counts, and every cilksort segment byte-identical to a
+    plain sort of its input (the check of examples/cilksort/cilksort.cu:225-258,
+    h == gold).  The segmented sort runs on the device: each key is tagged
+    with its segment index in the high 32 bits, so one sort of the tagged keys
+    sorts every segment in place."""
     import torch
     from tests import oracle_lib as orc
     ok = all(r.status == gt.ROOT_DONE for r in res)
@@ -527,24 +569,134 @@ def verify(gt, mix, res, src, arr):
             ok &= r.value == orc.fib(p) and r.tasks == orc.fib_tasks(p, 0)
         elif k == 1:
             ok &= r.value == orc.nq(p) and r.tasks == orc.nq_tasks(p, p - 1)
-    # sorted segments: non-decreasing inside every segment and same int64 sum
-    a = arr.long()
-    s = src.long()
-    d = a[1:] >= a[:-1]
-    bounds = torch.from_numpy(mix.offsets[1:-1] - 1).cuda() if len(mix.offsets) > 2 else None
-    if bounds is not None:
-        bounds = bounds[(bounds >= 0) & (bounds < len(d))]
-        d[bounds] = True
-    ok &= bool(d.all().item())
-    seg = torch.from_numpy(np.repeat(np.arange(mix.n), np.diff(mix.offsets))).cuda()
-    sa = torch.zeros(mix.n, dtype=torch.int64, device="cuda").index_add_(0, seg, a)
-    ss = torch.zeros(mix.n, dtype=torch.int64, device="cuda").index_add_(0, seg, s)
-    ok &= bool(torch.equal(sa, ss))
-    # a few segments exactly against a full sort
-    for i in np.nonzero(mix.kind == 2)[0][:8]:
-        o, n = int(mix.offsets[i]), int(mix.param[i])
-        ok &= bool(torch.equal(arr[o:o + n], torch.sort(src[o:o + n]).values))
+    nk = mix.total_keys
+    if nk:
+        sizes = torch.from_numpy(np.diff(mix.offsets)).cuda()
+        seg = torch.repeat_interleave(torch.arange(mix.n, device="cuda", dtype=torch.int64), sizes)
+        tagged = (seg << 32) | (src[:nk].long() + (1 << 31))
+        del seg
+        want = (torch.sort(tagged).values & 0xFFFFFFFF) - (1 << 31)
+        del tagged
+        ok &= bool(torch.equal(want.int(), arr[:nk]))
+        del want
+        torch.cuda.empty_cache()
     return bool(ok)
+
+
+def measure_per_root(gt, roots, res_batch, batched_value, tuned_overrides):
+    """The plain per-root baseline: gtap_reset-style relaunch per root
+    (gtap_launch_per_root), one pass over the mix, under the better of the
+    library defaults and the batch-tuned configuration."""
+    import torch
+    best = None
+    for label, ov in (("library defaults", {}), ("batch-tuned", dict(tuned_overrides))):
+        gt.gtap_finalize()
+        gt.gtap_initialize(gt.default_config(**ov))
+        gt.launch(roots[:64], per_root=True)          # warm
+        torch.cuda.synchronize()
+        p0 = time.perf_counter()
+        res_pr, st_pr = gt.launch(roots, per_root=True)
+        torch.cuda.synchronize()
+        pr_s = time.perf_counter() - p0
+        ok = all(a.value == b.value and a.status == b.status and a.tasks == b.tasks
+                 for a, b in zip(res_pr, res_batch))
+        tps = sum(r.tasks for r in res_pr) / pr_s
+        e = {"config": label, "tasks_per_s": tps, "s_per_step": pr_s, "kernel_ms_sum": st_pr.kernel_ms,
+             "results_match": ok}
+        if best is None or tps > best["tasks_per_s"]:
+            best = e
+    gt.gtap_finalize()
+    best["speedup_batched_vs_per_root"] = batched_value / best["tasks_per_s"]
+    return best
+
+
+def measure_reference_gpu(gt, reps=12):
+    """fib(30) and fib(34) with serial cutoff 12 on the reference GTaP GPU
+    build (oracle/_ref/fib_ref, fib_ref_c12: the reference runtime compiled
+    from its own headers with the hand-lowered fib, at its evaluation
+    geometry), beside this runtime's built-in fib (library defaults and the
+    autotuned configuration) and the pragma program lowered by
+    gtap_b200.lower in both result schemes.  Each time is the median CUDA-event
+    time of the persistent launch over `reps` launches (the first dropped);
+    every run's result is checked."""
+    import subprocess as sp
+    from tests import oracle_lib as orc
+    ref_dir = os.path.join(ROOT, "oracle", "_ref")
+    pragma_dir = os.path.join(ROOT, "tests", "pragma", "bin")
+
+    def run_exe(exe, n, cutoff):
+        r = sp.run([exe, str(n), str(cutoff), str(reps)], capture_output=True, text=True, timeout=120)
+        if r.returncode != 0:
+            return None, "exit %d" % r.returncode
+        d = json.loads(r.stdout.strip().splitlines()[-1])
+        vals = d.get("results", [d.get("result")])
+        if any(v != orc.fib(n) for v in vals) or d.get("error_code", 0) != 0:
+            return None, "wrong result"
+        return statistics.median(d["ms"][1:]), None
+
+    out = {}
+    for name, n, cutoff, ref_exe, tuned in (("fib30", 30, 0, "fib_ref", "b200_fib30.json"),
+                                            ("fib34_cutoff12", 34, 12, "fib_ref_c12", "b200_fib34c12.json")):
+        e = {"ms": {}, "notes": {}}
+        exe = os.path.join(ref_dir, ref_exe)
+        if os.path.exists(exe):
+            ms, err = run_exe(exe, n, cutoff)
+            e["ms"]["reference_build"] = ms
+            if err:
+                e["notes"]["reference_build"] = err
+        else:
+            e["notes"]["reference_build"] = "not built (oracle/Makefile ref-gpu needs the reference sources)"
+        for label, ov in (("builtin_defaults", {}),
+                          ("builtin_tuned", load_tuned(os.path.join(ROOT, "gtap_b200", "tuned", tuned)))):
+            gt.gtap_initialize(gt.default_config(**ov))
+            try:
+                ms = []
+                for _ in range(reps):
+                    res, st = gt.launch([gt.fib_root(n, cutoff)])
+                    assert res[0].value == orc.fib(n) and res[0].tasks == orc.fib_tasks(n, cutoff)
+                    ms.append(st.kernel_ms)
+                e["ms"][label] = statistics.median(ms[1:])
+            finally:
+                gt.gtap_finalize()
+        for label, b in (("lowered_retain", "fib_pragma"), ("lowered_parent", "fib_pragma_parent")):
+            exe = os.path.join(pragma_dir, b)
+            if os.path.exists(exe):
+                ms, err = run_exe(exe, n, cutoff)
+                e["ms"][label] = ms
+                if err:
+                    e["notes"][label] = err
+        ref_ms = e["ms"].get("reference_build")
+        if ref_ms:
+            e["speedup_vs_reference_build"] = {k: ref_ms / v for k, v in e["ms"].items()
+                                               if v and k != "reference_build"}
+        if not e["notes"]:
+            del e["notes"]
+        out[name] = e
+    return out
+
+
+def atomic_view(counters, mix, res, k_ms):
+    """L2 atomics the scheduler needs per launch, over the kernel time, against
+    the measured peak rate of scattered 32-bit atomic adds with a return value
+    (profiles/atomic_peak.json, written by gtap_measure_atomic_rate).  Counted:
+    one join-counter decrement per task that has a waiting parent (fib and
+    cilksort tasks other than roots), one CAS per own-deque pop and per steal,
+    one add per published batch, one per root-counter flush; the per-warp
+    batching keeps the last two small."""
+    joins = 0
+    for i, r in enumerate(res):
+        if int(mix.kind[i]) in (0, 2):
+            joins += r.tasks - 1
+    ops = joins + counters.get("pops", 0) + counters.get("steal_successes", 0) + counters.get("rounds", 0)
+    achieved = ops / (k_ms / 1e3) / 1e9
+    peak = None
+    try:
+        peak = json.load(open(os.path.join(ROOT, "profiles", "atomic_peak.json")))["scattered_atom_add_gops"]
+    except Exception:
+        pass
+    return {"bound": "l2_atomics", "achieved": achieved, "unit": "Gatom/s", "ops_per_launch": ops,
+            "peak": peak, "frac": (achieved / peak) if peak else None,
+            "peak_source": "measured (profiles/atomic_peak.json)" if peak else None}
 
 
 def measure_e2e(gt, mix, steps, tasks_per_step, world, arr_dev):

@@ -41,7 +41,7 @@ ERROR_INVALID_ARGUMENT = 11
 ERROR_NOT_INITIALIZED = 12
 
 STAT_NAMES = ["tasks", "executions", "rounds", "steal_attempts", "steal_successes", "stolen_tasks", "pops",
-              "published", "idle_polls", "overflow_pushes", "join_finishes"]
+              "published", "idle_polls", "overflow_pushes", "join_finishes", "idle_ns"]
 STAT_COUNT = 16
 
 
@@ -131,6 +131,8 @@ _SIGS = [
     ("gtap_selftest_queues", ctypes.c_int,
      [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32] + [ctypes.POINTER(ctypes.c_int64)] * 4),
     ("gtap_get_arena_counters", ctypes.c_int, [ctypes.POINTER(ctypes.c_int64), ctypes.c_int32]),
+    ("gtap_debug_set_ring_position", ctypes.c_int, [ctypes.c_int32, ctypes.c_uint32]),
+    ("gtap_measure_atomic_rate", ctypes.c_int, [ctypes.c_int32, ctypes.c_int64, ctypes.POINTER(ctypes.c_double)]),
     ("gtap_launch_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]),
     # support of the drop-in task-ABI header for caller-launched kernels
     ("gtap_external_initialize", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
@@ -330,6 +332,20 @@ def arena_counters():
     _check(lib().gtap_get_arena_counters(out, 8), "gtap_get_arena_counters")
     keys = ("fresh_next", "fresh_base", "pool", "overflow_left", "completed", "total_ids", "workers", "status")
     return dict(zip(keys, list(out)))
+
+
+def set_ring_position(position, target=0):
+    """Testing aid: both global rings empty, cursors at `position` (0..2^32-1).
+    target 0 = the gtap_initialize arena, 1 = gtap_launch_noalloc's scratch."""
+    _check(lib().gtap_debug_set_ring_position(target, position & 0xFFFFFFFF), "gtap_debug_set_ring_position")
+
+
+def measure_atomic_rate(mode=0, ops=1 << 28):
+    """Peak scattered 32-bit atomic adds per second (mode 0: atom.add with a
+    return value; 1: red.add)."""
+    v = ctypes.c_double(0.0)
+    _check(lib().gtap_measure_atomic_rate(mode, ops, ctypes.byref(v)), "gtap_measure_atomic_rate")
+    return v.value
 
 
 def selftest_queues(rounds=60, per_round_max=32, mode=7):

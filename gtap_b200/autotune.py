@@ -31,7 +31,7 @@ import time
 
 SPACE = {
     "warps_per_sm": [4, 8, 12, 16, 24, 32],
-    "block": [64, 128, 256, 512, 1024],
+    "block": [32, 64, 128, 256, 512, 1024],
     "deque_capacity": [256, 1024, 4096, 8192],
     "steal_batch": [1, 8, 32],
     "probe_width": [1, 4, 16, 32],

@@ -22,7 +22,8 @@ NVCC_FLAGS = [
 
 
 def sources():
-    return [os.path.join(CSRC, "gtap_capi.cu"), os.path.join(CSRC, "gtap_noalloc.cu")]
+    return [os.path.join(CSRC, "gtap_capi.cu"), os.path.join(CSRC, "gtap_noalloc.cu"),
+            os.path.join(CSRC, "gtap_microbench.cu")]
 
 
 LOWERED = os.path.join(ROOT, "tests", "lowered")
@@ -70,6 +71,17 @@ PRAGMA_BUILDS = [
     ("bary_block_pragma.cu", "bary_block_pragma", "-DGTAP_GRID_SIZE=1184 -DGTAP_BLOCK_SIZE=128"),
     ("fib_queues_pragma.cu", "fib_queues_pragma",
      "-DGTAP_GRID_SIZE=888 -DGTAP_BLOCK_SIZE=128 -DGTAP_MAX_CHILD_TASKS=2 -DGTAP_NUM_QUEUES=3"),
+    # the same thread-mode programs lowered with results delivered into the
+    # parent's frame (lower.py --results parent)
+    ("fib_pragma.cu", "fib_pragma_parent", "-DGTAP_GRID_SIZE=888 -DGTAP_BLOCK_SIZE=128 -DGTAP_MAX_CHILD_TASKS=2",
+     "parent"),
+    ("walk_pragma.cu", "walk_pragma_parent", "-DGTAP_GRID_SIZE=888 -DGTAP_BLOCK_SIZE=128", "parent"),
+    ("fib_queues_pragma.cu", "fib_queues_pragma_parent",
+     "-DGTAP_GRID_SIZE=888 -DGTAP_BLOCK_SIZE=128 -DGTAP_MAX_CHILD_TASKS=2 -DGTAP_NUM_QUEUES=3", "parent"),
+    ("cilksort_pragma.cu", "cilksort_pragma_parent",
+     "-DGTAP_GRID_SIZE=592 -DGTAP_BLOCK_SIZE=128 -DGTAP_MAX_CHILD_TASKS=4", "parent"),
+    ("bary_tree_pragma.cu", "bary_tree_pragma_parent",
+     "-DGTAP_GRID_SIZE=888 -DGTAP_BLOCK_SIZE=128 -DGTAP_MAX_CHILD_TASKS=8", "parent"),
 ]
 
 
@@ -82,7 +94,9 @@ def build_pragma(force=False):
     nvcc = os.environ.get("NVCC", "nvcc")
     header_deps = deps() + [os.path.join(HERE, "lower.py")]
     outs = []
-    for src, name, defs in PRAGMA_BUILDS:
+    for entry in PRAGMA_BUILDS:
+        src, name, defs = entry[:3]
+        results = entry[3] if len(entry) > 3 else "retain"
         s = os.path.join(PRAGMA_DIR, src)
         out = os.path.join(PRAGMA_BIN, name)
         outs.append(out)
@@ -91,7 +105,7 @@ def build_pragma(force=False):
             continue
         low = os.path.join(PRAGMA_BIN, name + "_lowered.cu")
         with open(s) as f:
-            text = lower_source(f.read())
+            text = lower_source(f.read(), results=results)
         with open(low, "w") as f:
             f.write(text)
         cmd = ([nvcc, "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",

@@ -82,10 +82,9 @@ static __device__ int ring_pop_one(const Arena& A, const Ring& r) {
         const unsigned avail = t - h;
         if (avail == 0 || avail > cap) return -1;
         if (atom_cas_relaxed(r.head, h, h + 1u) == h) {
-            const unsigned want = ring_tag(r, h);
             for (int spins = 0; spins <= (1 << 20); ++spins) {
                 const unsigned long long w = ld_acquire(&r.slots[h & (cap - 1)]);
-                if ((unsigned)(w >> 32) == want) return (int)(unsigned)(w & 0xFFFFFFFFu) - 1;
+                if (ring_word_ready(w, h, r.cap_log2)) return ring_word_value(w);
                 __nanosleep(64);
             }
             GTAP_ERROR(A, ERR_TIMEOUT, -1, -1, (int)h, 0);
@@ -649,6 +648,8 @@ __device__ void block_worker(const Arena& A, BlockShared& S, int* smem, int init
     unsigned long long t_watch = global_ns();
     unsigned seen_done = 0;
     int round = 0;
+    bool idle = false;                       // thread 0: in an idle stretch
+    unsigned long long idle_since = 0;       // thread 0: since when
     __syncthreads();
     for (;;) {
         GTAP_BPHASE(ph0);
@@ -673,6 +674,8 @@ __device__ void block_worker(const Arena& A, BlockShared& S, int* smem, int init
                 int stop = 0;
                 if (t < 0) {
                     S.st[GTAP_STAT_IDLE_POLLS] += 1;
+                    if (!idle) idle_since = global_ns();
+                    idle = true;
                     bt_bal_flush_all(A, S);
                     if (S.having) {
                         bt_prof_having(A, S);
@@ -701,6 +704,10 @@ __device__ void block_worker(const Arena& A, BlockShared& S, int* smem, int init
                     __nanosleep(32u << backoff);
                 } else {
                     backoff = 0;
+#ifndef GTAP_PHASE_TIMERS
+                    if (idle) S.st[GTAP_STAT_IDLE_NS] += global_ns() - idle_since;
+#endif
+                    idle = false;
                     if (!S.having) {
                         bt_prof_having(A, S);
                         S.having = 1;
@@ -713,6 +720,9 @@ __device__ void block_worker(const Arena& A, BlockShared& S, int* smem, int init
                         }
                     }
                 }
+#ifndef GTAP_PHASE_TIMERS
+                if (stop && idle) S.st[GTAP_STAT_IDLE_NS] += global_ns() - idle_since;
+#endif
                 S.stop = stop;
                 S.task = t;
                 S.nrel = 0;

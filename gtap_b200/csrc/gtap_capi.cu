@@ -49,7 +49,6 @@ struct Runtime {
     int external_workers = 0;   // workers of a kernel the caller launches (drop-in header), 0 = none
     int warps_per_block = 0;
     size_t smem_bytes = 0;
-    unsigned epoch = 0;
 
     // arena pieces
     char* records = nullptr;
@@ -197,10 +196,11 @@ __global__ void reset_kernel(Arena A, unsigned* counters, int n_roots, int fresh
     }
     if (tid == 0) {
         counters[kCtrFresh] = (unsigned)fresh_base;
-        counters[kCtrOvHead] = 0;
-        counters[kCtrOvTail] = 0;
-        counters[kCtrPoolHead] = 0;
-        counters[kCtrPoolTail] = 0;
+        // the rings keep their positions across launches (slot tags are
+        // lap numbers, gtap_ring.h): whatever is still queued is dropped by
+        // moving each consumer cursor to its producer cursor
+        counters[kCtrOvHead] = counters[kCtrOvTail];
+        counters[kCtrPoolHead] = counters[kCtrPoolTail];
         counters[kCtrNextRoot] = 0;
         counters[kCtrCompleted] = 0;
         counters[kCtrStatus] = 0;
@@ -241,12 +241,10 @@ Arena make_arena(int n_roots, int mode, int workers) {
     A.overflow.head = g.counters + kCtrOvHead;
     A.overflow.tail = g.counters + kCtrOvTail;
     A.overflow.cap_log2 = g.overflow_log2;
-    A.overflow.epoch = g.epoch;
     A.idpool.slots = g.ring_slots + (1ull << g.overflow_log2);
     A.idpool.head = g.counters + kCtrPoolHead;
     A.idpool.tail = g.counters + kCtrPoolTail;
     A.idpool.cap_log2 = g.idpool_log2;
-    A.idpool.epoch = g.epoch;
     A.fresh_next = g.counters + kCtrFresh;
     A.roots = g.d_roots;
     A.results = g.d_results;
@@ -382,7 +380,6 @@ int launch_resident(int n_roots, cudaStream_t s, float* ms_out, bool light) {
         GT_CUDA(cudaMemsetAsync(g.prof_working, 0, n * sizeof(long long), s));
         GT_CUDA(cudaMemsetAsync(g.prof_tasks, 0, n * sizeof(int), s));
     }
-    if ((++g.epoch & 0xFFFFu) == 0) ++g.epoch;   // epoch 0 would match never-written ring slots
 #ifdef GTAP_DEBUG_IDS
     GT_CUDA(cudaMemsetAsync(g.dbg, 0, (size_t)2 * g.cfg.total_ids * sizeof(int), s));
     GT_CUDA(cudaMemsetAsync(g.dbg + 2 * g.cfg.total_ids, 0xFF,
@@ -553,7 +550,6 @@ static int initialize_impl(const gtap_config* cfg_in, int external_workers) {
     GT_CUDA(cudaHostGetDevicePointer(&g.d_report, g.h_report, 0));
     int rc = ensure_root_capacity(4096);
     if (rc) return rc;
-    g.epoch = 1;
     g.initialized = true;
     GT_CUDA(cudaDeviceSynchronize());
     return 0;
@@ -578,7 +574,6 @@ int gtap_reset(void) {
     if (!g.initialized) return GTAP_ERROR_NOT_INITIALIZED;
     if (g.serving) return GTAP_ERROR_BUSY;
     if (g.h_report) memset(g.h_report, 0, sizeof(GtapErrorReport));
-    if ((++g.epoch & 0xFFFFu) == 0) ++g.epoch;   // epoch 0 would match never-written ring slots
     Arena A = make_arena(0, 0, g.workers);
     reset_kernel<<<64, 256>>>(A, g.counters, 0, g.workers * g.cfg.ids_per_worker);
     GT_CUDA(cudaGetLastError());
@@ -606,7 +601,6 @@ int gtap_external_prepare(void* arena_out, int64_t arena_bytes) {
         GT_CUDA(cudaMemset(g.prof_working, 0, n * sizeof(long long)));
         GT_CUDA(cudaMemset(g.prof_tasks, 0, n * sizeof(int)));
     }
-    if ((++g.epoch & 0xFFFFu) == 0) ++g.epoch;   // epoch 0 would match never-written ring slots
     const int W = g.external_workers;
     g.last_workers = W;
     g.last_block = false;
@@ -882,7 +876,6 @@ extern "C" int gtap_serve_start(int32_t ring_capacity, int32_t admit_watermark) 
     GT_CUDA(cudaEventCreate(&g.serve_ev0));
     GT_CUDA(cudaEventCreate(&g.serve_ev1));
     if (g.h_report) memset(g.h_report, 0, sizeof(GtapErrorReport));
-    if ((++g.epoch & 0xFFFFu) == 0) ++g.epoch;   // epoch 0 would match never-written ring slots
     // serve mode runs the light kernel (fib, n-queens, BFS and tree roots), or
     // the block kernel in block mode (every kind)
     const int W = block_mode() ? g.workers_block : g.workers_light;
@@ -1309,7 +1302,6 @@ extern "C" int gtap_selftest_queues(int32_t rounds, int32_t per_round_max, int32
     GT_CUDA(cudaMemset(ctr, 0, sizeof(SelftestCounters)));
     GT_CUDA(cudaMalloc(&sums, 2 * sizeof(unsigned long long)));
     GT_CUDA(cudaMemset(sums, 0, 2 * sizeof(unsigned long long)));
-    if ((++g.epoch & 0xFFFFu) == 0) ++g.epoch;   // epoch 0 would match never-written ring slots
     Arena A = make_arena(1, 0, W);
     reset_kernel<<<64, 256>>>(A, g.counters, 1, W * g.cfg.ids_per_worker);
     GT_CUDA(cudaGetLastError());
@@ -1335,6 +1327,37 @@ extern "C" int gtap_selftest_queues(int32_t rounds, int32_t per_round_max, int32
     int st = read_status();
     if (st) return st;
     return (dups == 0 && hc.bad_tokens == 0 && ones == (long long)hc.produced) ? 0 : GTAP_ERROR_QUEUE_OVERFLOW;
+}
+
+// ---------------------------------------------------------------------------
+// testing aid: ring positions
+// ---------------------------------------------------------------------------
+namespace gtap {
+int noalloc_set_ring_position(uint32_t position);   // gtap_noalloc.cu
+}
+
+extern "C" int gtap_debug_set_ring_position(int32_t target, uint32_t position) {
+    if (target == 1) {
+        std::lock_guard<std::mutex> lk(g_mu);
+        return gtap::noalloc_set_ring_position(position);
+    }
+    if (target != 0) return GTAP_ERROR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g.initialized) return GTAP_ERROR_NOT_INITIALIZED;
+    if (g.serving) return GTAP_ERROR_BUSY;
+    GT_CUDA(cudaDeviceSynchronize());
+    const unsigned pos[4] = {position, position, position, position};
+    // kCtrOvHead, kCtrOvTail, kCtrPoolHead, kCtrPoolTail are adjacent
+    static_assert(kCtrOvTail == kCtrOvHead + 1 && kCtrPoolHead == kCtrOvHead + 2 && kCtrPoolTail == kCtrOvHead + 3,
+                  "ring cursor slots");
+    GT_CUDA(cudaMemcpy(g.counters + kCtrOvHead, pos, sizeof(pos), cudaMemcpyHostToDevice));
+    // the slots are cleared too: a slot's tag is its position's lap, so a
+    // word left from before the jump could carry the tag of a position 2^32
+    // further on (continuous use rewrites every slot once per lap instead)
+    const size_t nslots = (1ull << g.overflow_log2) + (1ull << g.idpool_log2);
+    GT_CUDA(cudaMemset(g.ring_slots, 0, nslots * sizeof(unsigned long long)));
+    GT_CUDA(cudaDeviceSynchronize());
+    return 0;
 }
 
 // ---------------------------------------------------------------------------

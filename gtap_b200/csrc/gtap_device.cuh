@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/gtap_types.h"
+#include "gtap_ring.h"
 
 namespace gtap {
 
@@ -255,19 +256,16 @@ constexpr uint8_t kKindIndirect = 255;
 constexpr int kJoinCountMask = 0x00FFFFFF;
 
 // ---------------------------------------------------------------------------
-// MPMC ring of 32-bit values; each 64-bit slot = (lap << 32) | (value + 1)
+// MPMC ring of 32-bit values; each 64-bit slot = (lap + 1) << 32 | (value + 1)
+// (encoding and its invariants: gtap_ring.h).  The cursors keep counting
+// across launches; a launch starts with head moved to tail.
 // ---------------------------------------------------------------------------
 struct Ring {
     unsigned long long* slots;
     unsigned* head;       // consumer cursor
     unsigned* tail;       // producer cursor
     unsigned cap_log2;
-    unsigned epoch;       // distinguishes launches: tag = (epoch << 16 | lap) & 0xffffffff
 };
-
-__device__ __forceinline__ unsigned ring_tag(const Ring& r, unsigned pos) {
-    return ((r.epoch & 0xFFFFu) << 16) | ((pos >> r.cap_log2) & 0xFFFFu);
-}
 
 // ---------------------------------------------------------------------------
 // Arena: everything a launch needs, passed by value as the kernel parameter
@@ -399,8 +397,7 @@ static __device__ void ring_push_warp(const Arena& A, const Ring& r, int value, 
     (void)A;
     if ((int)lane < n) {
         unsigned p = pos + lane;
-        unsigned long long w = ((unsigned long long)ring_tag(r, p) << 32) | (unsigned)(value + 1);
-        st_relaxed(&r.slots[p & (cap - 1)], w);
+        st_relaxed(&r.slots[p & (cap - 1)], (unsigned long long)ring_word_of(p, r.cap_log2, value));
     }
 }
 
@@ -408,8 +405,7 @@ static __device__ void ring_push_warp(const Arena& A, const Ring& r, int value, 
 __device__ __forceinline__ void ring_push_one(const Ring& r, int value) {
     const unsigned cap = 1u << r.cap_log2;
     unsigned p = atom_add_relaxed(r.tail, 1u);
-    unsigned long long w = ((unsigned long long)ring_tag(r, p) << 32) | (unsigned)(value + 1);
-    st_relaxed(&r.slots[p & (cap - 1)], w);
+    st_relaxed(&r.slots[p & (cap - 1)], (unsigned long long)ring_word_of(p, r.cap_log2, value));
 }
 
 // Pop up to `want` values into lanes [0, got).  Slots reserved by a producer
@@ -433,12 +429,11 @@ static __device__ int ring_pop_warp(const Arena& A, const Ring& r, int want, int
     pos = __shfl_sync(0xffffffffu, pos, 0);
     if ((int)lane < got) {
         unsigned p = pos + lane;
-        unsigned want_tag = ring_tag(r, p);
         unsigned long long w = 0;
         int spins = 0;
         for (;;) {
             w = ld_acquire(&r.slots[p & (cap - 1)]);
-            if ((unsigned)(w >> 32) == want_tag) break;
+            if (ring_word_ready(w, p, r.cap_log2)) break;
             if (++spins > (1 << 20)) {
                 GTAP_ERROR(A, ERR_TIMEOUT, -1, -1, (int)p, 0);
                 w = 0;
@@ -446,7 +441,7 @@ static __device__ int ring_pop_warp(const Arena& A, const Ring& r, int want, int
             }
             __nanosleep(64);
         }
-        *value = (int)(unsigned)(w & 0xFFFFFFFFu) - 1;
+        *value = ring_word_value(w);
     }
     return got;
 }

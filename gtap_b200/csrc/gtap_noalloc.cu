@@ -27,16 +27,23 @@
 //     all workers, exceeds it; trees of up to a few hundred thousand tasks
 //     in all, or with serial cutoffs, fit.
 //
-// Set-up: the first call on a device, with that device current, looks up the
-// array's device address with cudaGetSymbolAddress (host code must not use
-// the symbol itself: on the host it only names a stand-in, and a kernel given
-// it would fault or read the wrong memory), sets the kernel's shared-memory
-// limit and sizes the grid.  Make that first call before any stream capture.
+// Set-up: the first call on a device, with that device current, sizes the
+// grid with an occupancy query.  Make that first call before any stream
+// capture.  Every call, with its device current, then looks up the array's
+// device address with cudaGetSymbolAddress (host code must not use the
+// symbol itself: on the host it only names a stand-in, and a kernel given it
+// would fault or read the wrong memory) and sets the kernel's shared-memory
+// limit.  Both are cheap and allocate nothing; redoing them each call keeps a
+// call correct after a cudaDeviceReset (a new context loads the module again,
+// possibly at another address) and after gtap_initialize() set a different
+// limit on the same kernel.
 //
-// Every call uses the same array and it keeps the previous call's contents;
-// each call clears what must start at zero.  Calls that overlap on the GPU
-// (two streams, or two host threads) race on the array and corrupt each
-// other: serialise them.
+// The call is synchronous: it returns once the launch has finished, with the
+// device status.  Calls from one process are serialised by a lock.  Every
+// call uses the same array and it keeps the previous call's contents; each
+// call clears what must start at zero.  Work that overlaps on the GPU and
+// bypasses that lock (two processes sharing a context, or device code of
+// another library writing the array) races on the array and corrupts it.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -46,6 +53,10 @@
 #include "gtap_programs.cuh"
 
 using namespace gtap;
+
+namespace gtap {
+int noalloc_set_ring_position(uint32_t position);   // testing aid, called by gtap_debug_set_ring_position
+}
 
 namespace {
 
@@ -83,10 +94,8 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
 
 struct DeviceSetup {
     bool ready = false;
-    unsigned char* base = nullptr;   // device address of g_noalloc_scratch
     int workers = 0;
     size_t smem = 0;
-    unsigned epoch = 0;
 };
 constexpr int kMaxDevices = 64;
 DeviceSetup g_setup[kMaxDevices];
@@ -114,18 +123,39 @@ __global__ void noalloc_reset_kernel(Arena A, unsigned* counters, int n_roots, i
         r.index = i;
         A.results[i] = r;
     }
-    for (int i = tid; i < kNoallocCounters; i += stride) counters[i] = (i == cFresh) ? (unsigned)fresh_base : 0u;
+    // the ring cursors keep counting across calls (gtap_ring.h): queued
+    // entries are dropped by moving each head to its tail
+    for (int i = tid; i < kNoallocCounters; i += stride) {
+        if (i == cOvTail || i == cPoolTail) continue;
+        counters[i] = (i == cFresh) ? (unsigned)fresh_base
+                      : (i == cOvHead) ? counters[cOvTail]
+                      : (i == cPoolHead) ? counters[cPoolTail] : 0u;
+    }
 }
 
-int setup_device(int dev, DeviceSetup& d) {
-    if (d.ready) return 0;
+const void* noalloc_kernel() {
+    return reinterpret_cast<const void*>(&thread_worker_kernel_lb<BuiltinProgramLight, 1>);
+}
+
+// Per call, with the device current: the array's device address in this
+// context, and the kernel's shared-memory limit (gtap_initialize sets the same
+// kernel's limit from its own configuration, which may be lower).
+int bind_scratch(unsigned char** base) {
     void* ptr = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
     if (e != cudaSuccess) return -(int)e;
-    const void* kfn = reinterpret_cast<const void*>(&thread_worker_kernel_lb<BuiltinProgramLight, 1>);
-    const size_t smem = noalloc_smem();
-    e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = cudaFuncSetAttribute(noalloc_kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)noalloc_smem());
     if (e != cudaSuccess) return -(int)e;
+    *base = static_cast<unsigned char*>(ptr);
+    return 0;
+}
+
+// Once per device: the grid (needs the shared-memory limit bound first).
+int setup_device(int dev, DeviceSetup& d) {
+    if (d.ready) return 0;
+    const void* kfn = noalloc_kernel();
+    const size_t smem = noalloc_smem();
+    cudaError_t e;
     int per_sm = 0, sms = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kNoallocBlock, smem);
     if (e != cudaSuccess) return -(int)e;
@@ -134,7 +164,6 @@ int setup_device(int dev, DeviceSetup& d) {
     if (per_sm < 1) return GTAP_ERROR_INVALID_ARGUMENT;
     const int wpb = kNoallocBlock / 32;
     const int blocks = std::min(std::min(per_sm, 2) * sms, kNoallocMaxWorkers / wpb);
-    d.base = static_cast<unsigned char*>(ptr);
     d.workers = blocks * wpb;
     d.smem = smem;
     d.ready = true;
@@ -142,6 +171,24 @@ int setup_device(int dev, DeviceSetup& d) {
 }
 
 }  // namespace
+
+// Testing aid behind gtap_debug_set_ring_position(1, pos): both rings empty
+// with their cursors at `position` (the caller holds the library lock).
+int gtap::noalloc_set_ring_position(uint32_t position) {
+    unsigned char* base = nullptr;
+    int rc = bind_scratch(&base);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    const unsigned pos[4] = {position, position, position, position};
+    static_assert(cOvTail == cOvHead + 1 && cPoolHead == cOvHead + 2 && cPoolTail == cOvHead + 3, "ring cursors");
+    cudaError_t e = cudaMemcpy(base + kOffCounters + sizeof(unsigned) * cOvHead, pos, sizeof(pos),
+                               cudaMemcpyHostToDevice);
+    // both rings' slots are cleared too (a word from before the jump could
+    // carry the lap tag of a position 2^32 further on)
+    if (e == cudaSuccess) e = cudaMemset(base + kOffRings, 0, ((size_t)2 << kNoallocRingLog2) * 8);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    return e == cudaSuccess ? 0 : -(int)e;
+}
 
 // See include/gtap.h.  No allocation: cudaGetSymbolAddress, attribute and
 // occupancy queries, two kernel launches, one 4-byte status read.
@@ -155,14 +202,14 @@ extern "C" int gtap_launch_noalloc(const gtap_root* d_roots, int32_t n_roots, gt
     if (e != cudaSuccess) return -(int)e;
     if (dev < 0 || dev >= kMaxDevices) return GTAP_ERROR_INVALID_ARGUMENT;
     DeviceSetup& d = g_setup[dev];
-    int rc = setup_device(dev, d);
+    unsigned char* base = nullptr;
+    int rc = bind_scratch(&base);
+    if (rc) return rc;
+    rc = setup_device(dev, d);
     if (rc) return rc;
 
-    unsigned char* base = d.base;
     unsigned* counters = reinterpret_cast<unsigned*>(base + kOffCounters);
     const int W = d.workers;
-    ++d.epoch;
-    if ((d.epoch & 0xFFFFu) == 0) ++d.epoch;   // ring tags of epoch 0 would match never-written slots
 
     Arena A{};
     A.num_workers = W;
@@ -191,12 +238,10 @@ extern "C" int gtap_launch_noalloc(const gtap_root* d_roots, int32_t n_roots, gt
     A.overflow.head = counters + cOvHead;
     A.overflow.tail = counters + cOvTail;
     A.overflow.cap_log2 = kNoallocRingLog2;
-    A.overflow.epoch = d.epoch;
     A.idpool.slots = rings + (1ull << kNoallocRingLog2);
     A.idpool.head = counters + cPoolHead;
     A.idpool.tail = counters + cPoolTail;
     A.idpool.cap_log2 = kNoallocRingLog2;
-    A.idpool.epoch = d.epoch;
     A.fresh_next = counters + cFresh;
     A.roots = d_roots;
     A.results = d_results;

@@ -173,10 +173,9 @@ static __device__ __noinline__ int alloc_id_slow(const Arena& A, WarpShared& S) 
         unsigned h = ld_relaxed(r.head), t = ld_relaxed(r.tail);
         if (t == h || t - h > cap) break;   // pool empty: every id is live
         if (atom_cas_relaxed(r.head, h, h + 1) == h) {
-            unsigned want = ring_tag(r, h);
             for (int spin = 0; spin < (1 << 20); ++spin) {
                 unsigned long long w = ld_acquire(&r.slots[h & (cap - 1)]);
-                if ((unsigned)(w >> 32) == want) return (int)(unsigned)(w & 0xFFFFFFFFu) - 1;
+                if (ring_word_ready(w, h, r.cap_log2)) return ring_word_value(w);
                 __nanosleep(64);
             }
             GTAP_ERROR(A, ERR_TIMEOUT, -1, -1, (int)h, 0);
@@ -882,6 +881,7 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
     int round = 0;
     int src_kind = 0;                        // debug builds: where this round's tasks came from
     bool idle = false;                       // counted in the hungry replicas
+    unsigned long long idle_since = 0;       // lane 0: start of the current idle stretch
     int* const hungry_mine = A.hungry + (S.worker % kHungryReplicas) * kHungryStride;
     auto hungry_add = [&](int d) {
         for (int r = 0; r < kHungryReplicas; ++r) red_add_relaxed_i32(A.hungry + r * kHungryStride, d);
@@ -926,6 +926,7 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
                 int stop = 0;
                 if (lane == 0) {
                     if (!idle && A.publish_lazy) hungry_add(1);
+                    if (!idle) idle_since = global_ns();
                     flush_all_bal(A, S);
                     S.st[GTAP_STAT_IDLE_POLLS] += 1;
                     if (ld_acquire(A.done_flag) != 0 || aborted(A)) stop = 1;
@@ -940,12 +941,20 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
                 }
                 idle = true;
                 stop = __shfl_sync(0xffffffffu, stop, 0);
-                if (stop) break;
+                if (stop) {
+#ifndef GTAP_PHASE_TIMERS
+                    if (lane == 0) S.st[GTAP_STAT_IDLE_NS] += global_ns() - idle_since;
+#endif
+                    break;
+                }
                 if (backoff < 6) ++backoff;
                 __nanosleep(32u << backoff);
                 continue;
             }
             if (idle && lane == 0 && A.publish_lazy) hungry_add(-1);
+#ifndef GTAP_PHASE_TIMERS
+            if (idle && lane == 0) S.st[GTAP_STAT_IDLE_NS] += global_ns() - idle_since;
+#endif
             idle = false;
             backoff = 0;
             if (!having) {

@@ -2,8 +2,9 @@
 
 The batched mix: `gtap_gen_mix(seed, n)` draws n roots, kind uniform over
 {fib, n-queens, cilksort}; fib n in [18, 28] without cutoff, n-queens n in
-[8, 11] with one task per row, cilksort of 2^e int32 keys with e uniform in
-[10, 20), keys = std::mt19937(per-root seed).  All cilksort roots share three
+[8, 11] with one task per row, cilksort of m * 2^e int32 keys with m uniform
+in [1024, 2048) and e uniform in [0, 9] (so sizes span 2^10 .. 2^20, log-
+uniform by octave), keys = std::mt19937(per-root seed).  All cilksort roots share three
 device slabs (source, sorted output, scratch); the leaves read the source, so
 a repeated launch needs no restore.
 """
@@ -15,7 +16,12 @@ SORT_CUTOFF, MERGE_CUTOFF = 64, 256   # examples/cilksort/cilksort.cu:10-11
 
 
 class Mix:
-    def __init__(self, gt, n_roots=N_ROOTS, seed=MIX_SEED):
+    """The seeded root mix.  `gen` supplies gen_mix(seed, n) and
+    gen_keys(seed, n): the library module (gtap_b200) or any object with the
+    same two generators."""
+
+    def __init__(self, gen, n_roots=N_ROOTS, seed=MIX_SEED):
+        gt = gen
         self.kind, self.param, self.seed = gt.gen_mix(seed, n_roots)
         sizes = np.where(self.kind == 2, self.param, 0).astype(np.int64)
         self.offsets = np.concatenate([[0], np.cumsum(sizes)])

@@ -127,6 +127,14 @@ int gtap_selftest_queues(int32_t rounds, int32_t per_round_max, int32_t mode, in
  * completed, out[5] arena ids, out[6] workers, out[7] status. */
 int gtap_get_arena_counters(int64_t* out, int32_t n);
 
+/* NEW, a testing aid with no counterpart in the reference.  Moves both cursors
+ * of both global rings (the overflow queue and the recycled-id pool) to
+ * `position`, leaving them empty, and clears their slots, so that a test
+ * reaches the 2^32 wrap of the cursors without 2^32 pushes first.  target 0: the arena of
+ * gtap_initialize() (between launches); target 1: the scratch array of
+ * gtap_launch_noalloc() on the current device (after its first call). */
+int gtap_debug_set_ring_position(int32_t target, uint32_t position);
+
 /* No counterpart in the reference.  For callers that cannot allocate device
  * memory (a serving loop that must avoid an allocation's implicit device-wide
  * synchronisation, or a process whose HBM already belongs to another
@@ -139,8 +147,10 @@ int gtap_get_arena_counters(int64_t* out, int32_t n);
  * 2^19 task records shared by live tasks and per-worker free-id caches (a
  * tree that outgrows them fails with GTAP_ERROR_TASK_ID_POOL_LOW_HEADROOM).
  * The first call on a device does a one-time set-up: make it before any
- * stream capture.  Calls share the array: calls that overlap on the GPU race
- * and must be serialised.  Synchronous; returns the device status. */
+ * stream capture.  Synchronous: returns once the launch has finished, with the
+ * device status.  Calls share the array; the library serialises the calls of
+ * one process with a lock, and GPU work that bypasses it (another process in
+ * the same context) races on the array. */
 int gtap_launch_noalloc(const gtap_root* d_roots, int32_t n_roots, gtap_root_result* d_results, void* stream);
 
 /* ------------------------------------------------------------------------ */
@@ -166,6 +176,14 @@ int gtap_external_error_code(int32_t* error_code);
 /* gtap_check_runtime_error() of the header (gtap_runtime_error.cuh:219): prints
  * the first device error, returns its code. */
 int gtap_external_check(void);
+
+/* Measurement aid (NEW, no reference counterpart): the peak rate, in
+ * operations per second, of 32-bit atomic adds to scattered words of an
+ * L2-resident 64 MiB table over a full grid -- mode 0 with a return value
+ * (atom.add, the join-counter decrement), mode 1 without (red.add).  At least
+ * ops (>= 2^20) operations per timed launch.  The denominator of the
+ * scheduler's atomic roofline. */
+int gtap_measure_atomic_rate(int32_t mode, int64_t ops, double* ops_per_s);
 
 /* Library version string (NEW). */
 const char* gtap_version(void);

@@ -137,6 +137,8 @@ enum {
     GTAP_STAT_IDLE_POLLS,         /* idle-loop iterations */
     GTAP_STAT_OVERFLOW_PUSHES,
     GTAP_STAT_JOIN_FINISHES,      /* block mode: continuations that only finish, booked at their join without running */
+    GTAP_STAT_IDLE_NS,            /* nanoseconds workers spent without a task (first failed acquire to the next
+                                     success or exit); idle fraction = this / (workers x kernel time) */
     GTAP_STAT_COUNT = 16
 };
 

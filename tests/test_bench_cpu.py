@@ -52,3 +52,28 @@ def test_mergesort_bytes_model():
     assert bench.mergesort_bytes(100, 128) == 800
     assert bench.mergesort_bytes(256, 128) == 8 * 256 * 2                 # one merge over two leaves
     assert bench.mergesort_bytes(1 << 24, 128) == 2415919104              # the 2^24-key workload's figure
+
+
+def test_reference_arm_runs_without_the_product_library():
+    """`bench.py --impl reference` builds the mix with the oracle's generators
+    and times the oracle's sequential programs: the product library is never
+    mapped into its process, and it prints the same `config` object as the
+    GPU arm (workload_config of the same mix built by the library)."""
+    import json
+    import subprocess
+    import sys
+    code = ("import sys, json, runpy; sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', "
+            "'--warmup', '1', '--roots', '96', '--cpu-sample-s', '0.2']; "
+            "runpy.run_path('bench.py', run_name='__main__'); "
+            "maps = open('/proc/self/maps').read(); "
+            "print(json.dumps({'lib_mapped': 'libgtap_b200' in maps, 'oracle_mapped': 'liboracle' in maps}))")
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-3000:]
+    lines = [json.loads(ln) for ln in out.stdout.strip().splitlines()]
+    line, maps = lines[0], lines[-1]
+    assert maps == {"lib_mapped": False, "oracle_mapped": True}
+    assert line["impl"] == "reference" and line["unit"] == "tasks/s" and line["value"] > 0
+    assert line["cpu_baseline"]["kind"] == "port" and line["e2e"]["h2d_bytes_per_step"] == 0
+    import gtap_b200 as gt
+    from gtap_b200.workloads import Mix
+    assert line["config"] == bench.workload_config(Mix(gt, 96))

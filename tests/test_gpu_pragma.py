@@ -1,7 +1,7 @@
 """Programs written with the gtap pragmas (tests/pragma), lowered by
 gtap_b200.lower and run on the B200 (B200 only): results must equal the
 oracle's (fib, n-queens), the sort must be ascending and a permutation of its
-input, the block-mode tree sum must equal its closed form, and the ternary
+input (thread-mode programs also in the --results parent lowering), the block-mode tree sum must equal its closed form, and the ternary
 walk (taskwaits inside if/else branches) must equal its recursion in Python;
 the probabilistic B-ary tree's mix sum and node count must equal the oracle's,
 in thread mode and in block mode."""
@@ -29,16 +29,23 @@ def run(exe, *args, timeout=180):
     return json.loads(r.stdout.strip().splitlines()[-1])
 
 
-@pytest.mark.parametrize("n,cutoff", [(0, 0), (1, 0), (2, 0), (20, 0), (27, 0), (30, 12)])
-def test_fib_pragma(bins, n, cutoff):
-    r = run(bins["fib_pragma"], n, cutoff, 2)
+# "_parent": the same program lowered with --results parent (children write
+# their results into the parent's frame)
+VARIANTS = ["", "_parent"]
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+@pytest.mark.parametrize("n,cutoff", [(0, 0), (1, 0), (2, 0), (20, 0), (27, 0), (30, 0), (30, 12)])
+def test_fib_pragma(bins, n, cutoff, variant):
+    r = run(bins["fib_pragma" + variant], n, cutoff, 2)
     assert r["error_code"] == 0
     assert r["results"] == [orc.fib(n)] * 2
 
 
+@pytest.mark.parametrize("variant", VARIANTS)
 @pytest.mark.parametrize("n,cutoff", [(0, 0), (2, 0), (22, 0), (29, 0), (32, 14)])
-def test_fib_queues_pragma(bins, n, cutoff):
-    r = run(bins["fib_queues_pragma"], n, cutoff, 2)
+def test_fib_queues_pragma(bins, n, cutoff, variant):
+    r = run(bins["fib_queues_pragma" + variant], n, cutoff, 2)
     assert r["error_code"] == 0 and r["queues"] == 3
     assert r["results"] == [orc.fib(n)] * 2
 
@@ -50,9 +57,10 @@ def test_nq_pragma(bins, n, cutoff):
     assert r["result"] == orc.nq(n)
 
 
+@pytest.mark.parametrize("variant", VARIANTS)
 @pytest.mark.parametrize("n", [1, 63, 1000, 100003, 1 << 20])
-def test_cilksort_pragma(bins, n):
-    r = run(bins["cilksort_pragma"], n, 7)
+def test_cilksort_pragma(bins, n, variant):
+    r = run(bins["cilksort_pragma" + variant], n, 7)
     assert r["error_code"] == 0
     assert r["sorted"] is True
 
@@ -96,9 +104,10 @@ def walk_expect(depth, ident):
     return (own * scale + b) & M64
 
 
+@pytest.mark.parametrize("variant", VARIANTS)
 @pytest.mark.parametrize("depth,ident", [(0, 5), (1, 0), (1, 1), (1, 2), (6, 0), (9, 1), (11, 2), (16, 0), (16, 4)])
-def test_walk_pragma(bins, depth, ident):
-    r = run(bins["walk_pragma"], depth, ident)
+def test_walk_pragma(bins, depth, ident, variant):
+    r = run(bins["walk_pragma" + variant], depth, ident)
     assert r["error_code"] == 0
     assert r["result"] == walk_expect(depth, ident)
 
@@ -107,9 +116,10 @@ def test_walk_pragma(bins, depth, ident):
     (0, 3, 4, 4, 10), (1, 3, 4, 4, 10), (6, 3, 8, 16, 12), (9, 4, 16, 32, 16), (15, 4, 8, 8, 16),
     (18, 4, 16, 64, 22),
 ])
-def test_bary_tree_pragma(bins, D, B, mem_ops, iters, log2n):
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_bary_tree_pragma(bins, D, B, mem_ops, iters, log2n, variant):
     seed = 7 + D
-    r = run(bins["bary_tree_pragma"], D, B, mem_ops, iters, log2n, seed, 2)
+    r = run(bins["bary_tree_pragma" + variant], D, B, mem_ops, iters, log2n, seed, 2)
     assert r["error_code"] == 0
     total, nodes = orc.bary_tree(D, B, mem_ops, iters, orc.bary_input(seed, 1 << log2n))
     assert r["nodes"] == nodes

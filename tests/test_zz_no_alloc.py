@@ -100,6 +100,50 @@ def test_noalloc_matches_gtap_launch_twice():
         assert np.array_equal(depth_na.cpu().numpy(), want_depth)
 
 
+def _noalloc_call(roots):
+    import torch
+    arr = (gt.Root * len(roots))(*roots)
+    d_roots = _device_bytes(arr)
+    d_results = torch.zeros(ctypes.sizeof(gt.RootResult) * len(roots), dtype=torch.uint8, device="cuda")
+    rc = gt.lib().gtap_launch_noalloc(ctypes.c_void_p(d_roots.data_ptr()), len(roots),
+                                      ctypes.c_void_p(d_results.data_ptr()), None)
+    return rc, (_results_from_device(d_results, len(roots)) if rc == 0 else None)
+
+
+def _small_roots_exact():
+    roots = [gt.fib_root(20), gt.fib_root(26, cutoff=10), gt.nq_root(9)]
+    rc, got = _noalloc_call(roots)
+    assert rc == 0, gt.gtap_get_runtime_error_string(rc)
+    assert [r.value for r in got] == [orc.fib(20), orc.fib(26), orc.nq(9)]
+    assert [r.tasks for r in got] == [orc.fib_tasks(20), orc.fib_tasks(26, 10), orc.nq_tasks(9, 8)]
+
+
+def test_noalloc_after_gtap_initialize_with_a_small_block():
+    """gtap_initialize sets the shared-memory limit of the same worker kernel
+    from its own configuration; a 32-thread block with a small staging buffer
+    lowers it below what the allocation-free entry point launches with.  The
+    entry point sets its limit on every call, so it keeps working."""
+    import torch
+    torch.cuda.init()
+    _small_roots_exact()
+    gt.gtap_initialize(gt.default_config(block=32, spawn_capacity=64))
+    gt.gtap_finalize()
+    _small_roots_exact()
+    _small_roots_exact()
+
+
+def test_noalloc_reports_an_outgrown_scratch_and_recovers():
+    """A tree whose live tasks outgrow the 2^19 records of the scratch array
+    (fib(34) without a cutoff, spread over every worker) ends with
+    GTAP_ERROR_TASK_ID_POOL_LOW_HEADROOM, a status the kernel returns, not a
+    fault; the next call starts from a clean scratch and is exact."""
+    import torch
+    torch.cuda.init()
+    rc, _ = _noalloc_call([gt.fib_root(34)])
+    assert rc == 6, rc
+    _small_roots_exact()
+
+
 def test_noalloc_rejects_too_many_roots():
     import torch
     torch.cuda.init()
