@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--tuned", default=TUNED, help="autotuner result whose overrides are applied first ('' = none)")
     ap.add_argument("--no-reference-gpu", dest="reference_gpu", action="store_false",
                     help="skip the fib comparison with the reference GTaP GPU build")
+    ap.add_argument("--no-extras", dest="extras", action="store_false",
+                    help="skip the reference's published configurations and the single-root BFS / tree runs")
     return ap.parse_args()
 
 
@@ -407,6 +409,12 @@ def main():
         gt.gtap_finalize()
         ref_gpu = measure_reference_gpu(gt)
 
+    published = single = None
+    if args.extras and rank == 0:
+        gt.gtap_finalize()
+        published = measure_published_configs(gt)
+        single = measure_single_roots(gt)
+
     cpu = None
     if not args.no_cpu and rank == 0 and world == 1:
         tasks_gpu = [r.tasks for r in res]
@@ -434,6 +442,7 @@ def main():
             "runtime": {"config": cfg.as_dict(), "tuned_from": tuned_from},
             "verified": verified, "gpu_launches": 2 * args.steps, "e2e": e2e, "roofline": roof,
             "cpu_baseline": cpu, "clocks": ck, "serve": serve, "block_mode": block, "mergesort_thread": msort,
+            "single_roots": single, "published_configs": published,
             "reference_gpu": ref_gpu, "per_root_launch": per_root, "scheduler": sched}
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -672,6 +681,97 @@ def measure_reference_gpu(gt, reps=12):
         if not e["notes"]:
             del e["notes"]
         out[name] = e
+    return out
+
+
+def measure_published_configs(gt, reps=5):
+    """The configurations the reference publishes numbers for (GH200,
+    evaluation/2-comparison/*/..._performance_results.csv), on this B200:
+    n-queens(13) with the reference program's cutoff depth 7 (gtap_nq.cu:66),
+    and thread-mode cilksort (cutoffs 64/256, gtap_cilksort.cu:11-12) of 10^7,
+    5*10^7 and 10^8 std::mt19937(42) keys standing in for gen_vector files.
+    Median CUDA-event kernel time; every result checked (the sorted keys
+    against a plain sort of the same keys on the device)."""
+    import torch
+    from tests import oracle_lib as orc
+    out = {}
+    gt.gtap_initialize(gt.default_config())
+    try:
+        ms = []
+        for _ in range(reps + 1):
+            res, st = gt.launch([gt.nq_root(13, 7)])
+            assert res[0].value == orc.nq(13) and res[0].tasks == orc.nq_tasks(13, 7)
+            ms.append(st.kernel_ms)
+        m = statistics.median(ms[1:])
+        out["nq13_cutoff7"] = {"ms": m, "tasks": int(res[0].tasks), "published_gh200_ms": 0.8505,
+                               "published_source": "evaluation/2-comparison/nq/nq_performance_results.csv:14",
+                               "gh200_over_b200": 0.8505 / m}
+        for n, pub, line in ((10 ** 7, 10.217, 8), (5 * 10 ** 7, 36.962, 10), (10 ** 8, 82.1875, 11)):
+            keys = orc.keys(42, n)
+            src = torch.from_numpy(keys).cuda()
+            arr = torch.empty_like(src)
+            tmp = torch.empty_like(src)
+            root = gt.cilksort_root(src.data_ptr(), arr.data_ptr(), tmp.data_ptr(), n, 64, 256)
+            ms = []
+            for _ in range(reps + 1):
+                res, st = gt.launch([root])
+                ms.append(st.kernel_ms)
+            ok = res[0].status == gt.ROOT_DONE and bool(torch.equal(arr, torch.sort(src).values))
+            m = statistics.median(ms[1:])
+            out["cilksort_thread_%d" % n] = {"ms": m, "keys_per_s": n / (m / 1e3), "sorted_equals_plain_sort": ok,
+                                             "published_gh200_ms": pub, "gh200_over_b200": pub / m,
+                                             "published_source": "evaluation/2-comparison/cilksort/"
+                                                                 "cilksort_performance_results.csv:%d" % line}
+            del src, arr, tmp
+            torch.cuda.empty_cache()
+    finally:
+        gt.gtap_finalize()
+    out["note"] = "published numbers are GH200 (sm_90): context for the same configurations, not a ratio claimed"
+    return out
+
+
+def measure_single_roots(gt, reps=3):
+    """One root per launch, library defaults: asynchronous BFS from the
+    highest-degree vertex of R-MAT graphs (scale 16/18/20, edge factor 16,
+    the serve workload's graphs) and int64 sums over unbalanced binary trees
+    (2^18 / 2^20 nodes).  BFS reports GTEPS = CSR edges / kernel time (every
+    edge is scanned once per relaxation of its source); depths are checked
+    against the oracle's queue BFS, sums exactly."""
+    import torch
+    from tests import oracle_lib as orc
+    out = {"bfs": [], "treesum": []}
+    gt.gtap_initialize(gt.default_config())
+    try:
+        for s in (16, 18, 20):
+            row, col = gt.gen_rmat(s, 16, 1000 + s)
+            src = gt.max_degree_vertex(row)
+            drow, dcol = torch.from_numpy(row).cuda(), torch.from_numpy(col).cuda()
+            nv = len(row) - 1
+            depth = torch.empty(nv, dtype=torch.int32, device="cuda")
+            root = gt.bfs_root(drow.data_ptr(), dcol.data_ptr(), depth.data_ptr(), nv, src, 32)
+            ms, tasks = [], 0
+            for _ in range(reps + 1):
+                depth.fill_(0x3f3f3f3f)
+                torch.cuda.synchronize()
+                res, st = gt.launch([root])
+                ms.append(st.kernel_ms)
+                tasks = int(res[0].tasks)
+            ok = bool(np.array_equal(depth.cpu().numpy(), orc.bfs(row, col, src)))
+            m = statistics.median(ms[1:])
+            out["bfs"].append({"scale": s, "vertices": nv, "edges": len(col), "ms": m,
+                               "gteps": len(col) / (m / 1e3) / 1e9, "tasks": tasks, "depths_ok": ok})
+        for n in (1 << 18, 1 << 20):
+            left, right, value, size = gt.gen_tree(n, 2000 + n)
+            arrs = [torch.from_numpy(a).cuda() for a in (left, right, value, size)]
+            ms = []
+            for _ in range(reps + 1):
+                res, st = gt.launch([gt.treesum_root(*[a.data_ptr() for a in arrs], n, 0, 32)])
+                ms.append(st.kernel_ms)
+            m = statistics.median(ms[1:])
+            out["treesum"].append({"nodes": n, "ms": m, "tasks": int(res[0].tasks),
+                                   "sum_ok": res[0].value == int(value.astype(np.int64).sum())})
+    finally:
+        gt.gtap_finalize()
     return out
 
 

@@ -49,6 +49,8 @@ struct Runtime {
     int external_workers = 0;   // workers of a kernel the caller launches (drop-in header), 0 = none
     int warps_per_block = 0;
     size_t smem_bytes = 0;
+    size_t smem_full = 0;       // thread_worker_kernel<BuiltinProgram>: smem_bytes + per-warp leaf buffers if they fit
+    int leaf_buf = 0;           // leaf input buffers per warp in smem_full
 
     // arena pieces
     char* records = nullptr;
@@ -165,8 +167,8 @@ cudaError_t launch_worker(const Arena& A, bool light, cudaStream_t s) {
     const bool one = g.cfg.num_queues == 1;
     if (light && one) thread_worker_kernel_lb<BuiltinProgramLight, 1><<<blocks, g.cfg.block, g.smem_bytes, s>>>(A);
     else if (light) thread_worker_kernel_lb<BuiltinProgramLight, kMaxQueues><<<blocks, g.cfg.block, g.smem_bytes, s>>>(A);
-    else if (one) thread_worker_kernel<BuiltinProgram, 1><<<blocks, g.cfg.block, g.smem_bytes, s>>>(A);
-    else thread_worker_kernel<BuiltinProgram, kMaxQueues><<<blocks, g.cfg.block, g.smem_bytes, s>>>(A);
+    else if (one) thread_worker_kernel<BuiltinProgram, 1><<<blocks, g.cfg.block, g.smem_full, s>>>(A);
+    else thread_worker_kernel<BuiltinProgram, kMaxQueues><<<blocks, g.cfg.block, g.smem_full, s>>>(A);
     return cudaGetLastError();
 }
 
@@ -276,6 +278,7 @@ Arena make_arena(int n_roots, int mode, int workers) {
     A.handle_meta = g.handle_meta;
     A.handle_cap = c.result_handles;
     A.staging = g.staging;
+    A.leaf_buf = g.leaf_buf;
     return A;
 }
 
@@ -477,10 +480,22 @@ static int initialize_impl(const gtap_config* cfg_in, int external_workers) {
     GT_CUDA(cudaGetDevice(&g.device));
     GT_CUDA(cudaDeviceGetAttribute(&g.sm_count, cudaDevAttrMultiProcessorCount, g.device));
     const size_t smem = smem_for(c);
+    // the sorting kernel also holds leaf buffers: per warp kLeafBatch input
+    // buffers and an output buffer, or fewer inputs when the block's shared
+    // memory cannot hold them
+    int smem_optin = 0;
+    GT_CUDA(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, g.device));
+    int leaf_buf = prog::kLeafBatch;
+    size_t smem_full = smem;
+    for (; leaf_buf > 0; leaf_buf /= 2) {
+        smem_full = smem + (size_t)(c.block / 32) * (leaf_buf + 1) * BuiltinProgram::kLeafKeys * sizeof(int);
+        if (smem_full <= (size_t)smem_optin) break;
+    }
+    if (leaf_buf == 0) smem_full = smem;
     int per_sm_full = 0, per_sm_light = 0;
-    GT_CUDA(cudaFuncSetAttribute(kernel_full(c.num_queues), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    GT_CUDA(cudaFuncSetAttribute(kernel_full(c.num_queues), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_full));
     GT_CUDA(cudaFuncSetAttribute(kernel_light(c.num_queues), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    GT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_full, kernel_full(c.num_queues), c.block, smem));
+    GT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_full, kernel_full(c.num_queues), c.block, smem_full));
     GT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_light, kernel_light(c.num_queues), c.block, smem));
     if (per_sm_light < 1) return GTAP_ERROR_INVALID_ARGUMENT;
     // one resident wave per variant; grid = 0 fills the GPU, otherwise cap it
@@ -515,6 +530,8 @@ static int initialize_impl(const gtap_config* cfg_in, int external_workers) {
     }
     g.cfg = c;
     g.smem_bytes = smem;
+    g.smem_full = smem_full;
+    g.leaf_buf = leaf_buf;
 
     const int stride = kHdrBytes + ((c.frame_bytes + 15) / 16) * 16;
     GT_CUDA(cudaMalloc(&g.records, (size_t)(c.total_ids + 1) * stride));   // + spare record for failed allocations

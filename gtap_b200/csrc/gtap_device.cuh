@@ -352,6 +352,7 @@ struct Arena {
     // buffers do not fit static shared memory: [workers][Q][spawn_cap + kLocalCap]
     int* staging;
     int handle_cap;
+    int leaf_buf;                      // leaf input buffers per warp at the end of dynamic shared memory (0: none)
 };
 
 // ---------------------------------------------------------------------------

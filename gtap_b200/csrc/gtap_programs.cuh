@@ -293,6 +293,97 @@ static __device__ __noinline__ void warp_merge(const int* a, int alen, const int
     }
 }
 
+// Leaves of at most kLeafKeys keys go through the warp's shared-memory leaf
+// buffers: up to kLeafBatch input buffers of kLeafKeys keys and one output
+// buffer.  The keys of a batch of leaves are copied in with cp.async (every
+// copy of every leaf of the batch in flight at once: one round trip per
+// batch, no registers held), merge-path searches and merges read shared
+// memory, and results leave with coalesced stores.  A merge leaf done in
+// global memory costs a dependent round trip per binary-search step and per
+// merged key, and leaves done one at a time a round trip each.  The loops
+// stay rolled: the mix runs these leaves beside fib and n-queens tasks on the
+// same SMs, which share the instruction cache with them.
+constexpr int kLeafKeys = 256;
+constexpr int kLeafBatch = 4;
+
+__device__ __forceinline__ void cp_async4(int* smem_dst, const int* gmem_src) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Starts copying buf[0, total) = a[0, alen) ++ b[0, total - alen); the
+// caller waits (cp_async_wait_all + __syncwarp) before reading buf.
+__device__ __forceinline__ void leaf_issue(const int* a, int alen, const int* b, int total, int* buf) {
+#pragma unroll 1
+    for (int i = (int)lane_id(); i < total; i += 32) cp_async4(buf + i, i < alen ? a + i : b + (i - alen));
+}
+
+// out[d, d + 8) (clipped to alen + blen) = outputs d.. of the merge of
+// sorted a[0, alen) and b[0, blen) (merge path; a's key first among equal keys).
+__device__ __forceinline__ void merge_path8(const int* a, int alen, const int* b, int blen, int d, int* out) {
+    int lo = max(0, d - blen), hi = min(d, alen);
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (a[mid] <= b[d - 1 - mid]) lo = mid + 1;
+        else hi = mid;
+    }
+    int i = lo, j = d - lo;
+    const int end = min(d + 8, alen + blen);
+#pragma unroll 1
+    for (int e = d; e < end; ++e) {
+        const bool take_a = j >= blen || (i < alen && a[i] <= b[j]);
+        out[e] = take_a ? a[i++] : b[j++];
+    }
+}
+
+__device__ __forceinline__ void leaf_store(const int* buf, int total, int* dst) {
+#pragma unroll 1
+    for (int i = (int)lane_id(); i < total; i += 32) dst[i] = buf[i];
+}
+
+// in = a[0, alen) ++ b[0, blen), both sorted: dst[0, alen + blen) = their
+// merge (the sequence warp_merge writes), through out.
+static __device__ __noinline__ void leaf_merge_out(const int* in, int alen, int blen, int* out, int* dst) {
+    __syncwarp();   // out's previous contents were stored already
+    const int d0 = (int)lane_id() * 8;
+    if (d0 < alen + blen) merge_path8(in, alen, in + alen, blen, d0, out);
+    __syncwarp();
+    leaf_store(out, alen + blen, dst);
+}
+
+// dst[0, n) = in[0, n) sorted: 64-key runs sorted in place by
+// warp_bitonic64, then merge passes of doubling width between in and out.
+static __device__ __noinline__ void leaf_sort_out(int* in, int n, int* out, int* dst) {
+    const int lane = (int)lane_id();
+    __syncwarp();   // out's previous contents were stored already
+#pragma unroll 1
+    for (int c = 0; c < n; c += 64) {
+        int v0 = c + lane < n ? in[c + lane] : 0x7fffffff;
+        int v1 = c + lane + 32 < n ? in[c + lane + 32] : 0x7fffffff;
+        warp_bitonic64(v0, v1);   // keys past n sort last and are never stored
+        if (c + lane < n) in[c + lane] = v0;
+        if (c + lane + 32 < n) in[c + lane + 32] = v1;
+    }
+    __syncwarp();
+    int* from = in;
+    int* to = out;
+#pragma unroll 1
+    for (int w = 64; w < n; w <<= 1) {
+        const int d0 = lane * 8;
+        if (d0 < n) {
+            const int s = d0 / (2 * w) * (2 * w);
+            const int alen = min(w, n - s), blen = min(w, n - s - alen);
+            merge_path8(from + s, alen, from + s + alen, blen, d0 - s, to + s);
+        }
+        __syncwarp();
+        int* t = from;
+        from = to;
+        to = t;
+    }
+    leaf_store(from, n, dst);
+}
+
 // out[0, n) = in[0, n) sorted; scr is n keys of scratch (in may alias out).
 // 64-key runs by warp_bitonic64, then merge passes of doubling width that
 // alternate between scr and out so the last one lands in out.
@@ -688,6 +779,7 @@ struct BuiltinProgramT {
     static constexpr int kFrameBytes = prog::kFrameBytes;
     static constexpr bool kFrameWords = true;    // exec gets the first 32 frame bytes
     static constexpr bool kFuncTable = false;    // kinds are dispatched by the switch below
+    static constexpr int kLeafKeys = kSorts ? prog::kLeafKeys : 0;   // keys per leaf buffer (0: no warp leaves)
 
     __device__ static int root_kind(int k) {
         switch (k) {
@@ -772,31 +864,80 @@ struct BuiltinProgramT {
 
     // Leaf work of the lanes in `mask`, done by the whole warp: each marked
     // lane's task kind and frame words (loaded with its header this round)
-    // are broadcast, and the warp sorts or merges for that task.
+    // are broadcast, and the warp sorts or merges for that task.  Leaves of
+    // at most kLeafKeys keys go in batches through the leaf buffers (S.lbuf:
+    // A.leaf_buf input buffers and one output buffer), larger ones one at a
+    // time through global memory.
+    struct LeafArgs {
+        int k, z1, q1;
+        int *p0, *p1, *p2;
+    };
+    __device__ static LeafArgs leaf_args(int l, int kind, const int4& w0, const int4& w1) {
+        LeafArgs a;
+        a.k = __shfl_sync(prog::kFull, kind, l);
+        const unsigned x0 = (unsigned)__shfl_sync(prog::kFull, w0.x, l), y0 = (unsigned)__shfl_sync(prog::kFull, w0.y, l);
+        const unsigned z0 = (unsigned)__shfl_sync(prog::kFull, w0.z, l), q0 = (unsigned)__shfl_sync(prog::kFull, w0.w, l);
+        const unsigned x1 = (unsigned)__shfl_sync(prog::kFull, w1.x, l), y1 = (unsigned)__shfl_sync(prog::kFull, w1.y, l);
+        a.z1 = __shfl_sync(prog::kFull, w1.z, l);
+        a.q1 = __shfl_sync(prog::kFull, w1.w, l);
+        a.p0 = reinterpret_cast<int*>((unsigned long long)x0 | ((unsigned long long)y0 << 32));
+        a.p1 = reinterpret_cast<int*>((unsigned long long)z0 | ((unsigned long long)q0 << 32));
+        a.p2 = reinterpret_cast<int*>((unsigned long long)x1 | ((unsigned long long)y1 << 32));
+        return a;
+    }
     __device__ static void warp_leaves(const Arena& A, WarpShared& S, unsigned mask, int kind, const int4& w0,
                                        const int4& w1) {
-        (void)A;
-        (void)S;
         if constexpr (kSorts) {
-        while (mask) {
-            const int l = __ffs(mask) - 1;
-            mask &= mask - 1;
-            const int k = __shfl_sync(prog::kFull, kind, l);
-            const unsigned x0 = (unsigned)__shfl_sync(prog::kFull, w0.x, l), y0 = (unsigned)__shfl_sync(prog::kFull, w0.y, l);
-            const unsigned z0 = (unsigned)__shfl_sync(prog::kFull, w0.z, l), q0 = (unsigned)__shfl_sync(prog::kFull, w0.w, l);
-            const unsigned x1 = (unsigned)__shfl_sync(prog::kFull, w1.x, l), y1 = (unsigned)__shfl_sync(prog::kFull, w1.y, l);
-            const int z1 = __shfl_sync(prog::kFull, w1.z, l), q1 = __shfl_sync(prog::kFull, w1.w, l);
-            int* p0 = reinterpret_cast<int*>((unsigned long long)x0 | ((unsigned long long)y0 << 32));
-            int* p1 = reinterpret_cast<int*>((unsigned long long)z0 | ((unsigned long long)q0 << 32));
-            int* p2 = reinterpret_cast<int*>((unsigned long long)x1 | ((unsigned long long)y1 << 32));
-            switch (k) {
-                case prog::K_CILKSORT: prog::warp_sort(p2, p0, p1, z1); break;   // src -> arr, tmp scratch
-                case prog::K_CILKMERGE: prog::warp_merge(p0, z1, p1, q1, p2); break;   // a, b -> dst
-                case prog::K_MERGESORT: prog::warp_sort(p0, p1, p2, z1); break;   // in -> out, tmp scratch
-                default: break;
+            const unsigned lane = lane_id();
+            int* buf = S.lbuf;
+            const int nbuf = buf ? A.leaf_buf : 0;
+            // frames: cilksort {arr, tmp, src, n}, cilkmerge {a, b, dst, alen, blen}, mergesort {in, out, tmp, n}
+            bool small = false;
+            if (nbuf > 0 && ((mask >> lane) & 1u))
+                small = kind == prog::K_CILKMERGE ? w1.z + w1.w <= prog::kLeafKeys : w1.z <= prog::kLeafKeys;
+            unsigned batch_of = __ballot_sync(prog::kFull, small);
+            unsigned big = mask & ~batch_of;
+            while (big) {
+                const int l = __ffs(big) - 1;
+                big &= big - 1;
+                const LeafArgs a = leaf_args(l, kind, w0, w1);
+                switch (a.k) {
+                    case prog::K_CILKSORT: prog::warp_sort(a.p2, a.p0, a.p1, a.z1); break;   // src -> arr, tmp scratch
+                    case prog::K_CILKMERGE: prog::warp_merge(a.p0, a.z1, a.p1, a.q1, a.p2); break;   // a, b -> dst
+                    case prog::K_MERGESORT: prog::warp_sort(a.p0, a.p1, a.p2, a.z1); break;   // in -> out, tmp scratch
+                    default: break;
+                }
             }
-        }
+            int* out = buf + (size_t)nbuf * prog::kLeafKeys;
+            while (batch_of) {
+                unsigned grp = 0;
+                for (int c = 0; c < nbuf && batch_of; ++c) {
+                    grp |= batch_of & (0u - batch_of);
+                    batch_of &= batch_of - 1;
+                }
+                __syncwarp();   // the input buffers' previous contents are no longer read
+                int j = 0;
+                for (unsigned g = grp; g; g &= g - 1, ++j) {
+                    const LeafArgs a = leaf_args(__ffs(g) - 1, kind, w0, w1);
+                    int* in = buf + (size_t)j * prog::kLeafKeys;
+                    if (a.k == prog::K_CILKSORT) prog::leaf_issue(a.p2, a.z1, a.p2, a.z1, in);
+                    else if (a.k == prog::K_CILKMERGE) prog::leaf_issue(a.p0, a.z1, a.p1, a.z1 + a.q1, in);
+                    else prog::leaf_issue(a.p0, a.z1, a.p0, a.z1, in);
+                }
+                prog::cp_async_wait_all();
+                __syncwarp();
+                j = 0;
+                for (unsigned g = grp; g; g &= g - 1, ++j) {
+                    const LeafArgs a = leaf_args(__ffs(g) - 1, kind, w0, w1);
+                    int* in = buf + (size_t)j * prog::kLeafKeys;
+                    if (a.k == prog::K_CILKSORT) prog::leaf_sort_out(in, a.z1, out, a.p0);
+                    else if (a.k == prog::K_CILKMERGE) prog::leaf_merge_out(in, a.z1, a.q1, out, a.p2);
+                    else prog::leaf_sort_out(in, a.z1, out, a.p1);
+                }
+            }
         } else {
+            (void)A;
+            (void)S;
             (void)mask;
             (void)kind;
             (void)w0;

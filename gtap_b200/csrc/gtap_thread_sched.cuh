@@ -103,6 +103,7 @@ struct WarpShared {
     unsigned long long t_watch;
     int* sbuf;                 // [num_queues][spawn_cap] staged child ids (| spawner lane << 27)
     int* lstk;                 // [num_queues][kLocalCap] ready tasks not yet visible to thieves
+    int* lbuf;                 // leaf buffers: [A.leaf_buf + 1][Prog::kLeafKeys] (programs with warp leaves), or null
 };
 
 // Positions of this warp's local stacks and deques.  Only the scheduler
@@ -1288,12 +1289,13 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
 // created before the loop, e.g. by the drop-in __gtap_push_initial_task).
 template <class Prog, int QM>
 __device__ __forceinline__ void thread_worker_run(const Arena& A, WarpShared& S, int worker, int* sbuf, int* lstk,
-                                                  int initial_tid) {
+                                                  int initial_tid, int* lbuf = nullptr) {
     const unsigned lane = lane_id();
     if (lane == 0) {
         S.worker = worker;
         S.sbuf = sbuf;
         S.lstk = lstk;
+        S.lbuf = lbuf;
         for (int k = 0; k < kMaxQueues; ++k) S.cnt[k] = 0;
         S.alloc_last = 0;
         S.alloc_pos = 0;
@@ -1319,7 +1321,8 @@ __device__ __forceinline__ void thread_worker_run(const Arena& A, WarpShared& S,
     if ((int)lane < GTAP_STAT_COUNT) A.stats[(size_t)worker * GTAP_STAT_COUNT + lane] = S.st[lane];
 }
 
-// Kernel body: warps_per_block WarpShared records + staging buffers in dynamic smem.
+// Kernel body: warps_per_block WarpShared records + staging buffers in dynamic
+// smem, then (programs with warp leaves) A.leaf_buf + 1 leaf buffers per warp.
 template <class Prog, int QM>
 __device__ __forceinline__ void thread_worker_body(const Arena& A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1327,9 +1330,12 @@ __device__ __forceinline__ void thread_worker_body(const Arena& A) {
     WarpShared* ws = reinterpret_cast<WarpShared*>(smem_raw);
     int* sb_base = reinterpret_cast<int*>(smem_raw + sizeof(WarpShared) * A.warps_per_block);
     int* ls_base = sb_base + (size_t)A.warps_per_block * A.num_queues * A.spawn_cap;
+    int* lb_base = ls_base + (size_t)A.warps_per_block * A.num_queues * kLocalCap;
     thread_worker_run<Prog, QM>(A, ws[wib], blockIdx.x * A.warps_per_block + wib,
                             sb_base + (size_t)wib * A.num_queues * A.spawn_cap,
-                            ls_base + (size_t)wib * A.num_queues * kLocalCap, -1);
+                            ls_base + (size_t)wib * A.num_queues * kLocalCap, -1,
+                            (Prog::kLeafKeys && A.leaf_buf) ? lb_base + (size_t)wib * (A.leaf_buf + 1) * Prog::kLeafKeys
+                                                            : nullptr);
 }
 
 

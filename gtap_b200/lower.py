@@ -59,8 +59,8 @@ reads its frame from the words the worker loads with the task header
 (GTAP_FRAME_WORDS, __gtap_dispatch_words), working on a copy that is written
 back before a join.  Results then go to plain locals or parameters of the
 callee's return type, one per local and join, with no return between a spawn
-and its join; the entry kernel gets launch bounds that keep every worker
-resident.
+and its join.  In thread mode the entry kernel gets launch bounds that keep
+every worker resident (both result schemes).
 """
 import argparse
 import re
@@ -872,11 +872,13 @@ class Lowering:
 
     @staticmethod
     def _bound_kernel(head):
-        """--results parent: give the kernel that holds the entry launch bounds
-        asking for every worker block to be resident (GTAP_GRID_SIZE blocks over
-        148 SMs, at most 32 blocks and 2048 threads per SM), so the compiler
-        keeps the preloaded frame words without raising the register count past
-        what that residency allows."""
+        """Thread mode: give the kernel that holds the entry launch bounds
+        asking for every worker block to be resident (GTAP_GRID_SIZE blocks
+        over 148 SMs, at most 32 blocks and 2048 threads per SM).  A persistent
+        worker that is not resident only starts when a resident one exits, so
+        without the bounds a register-heavy program ran with fewer workers
+        than it launched; with --results parent the bounds also keep the
+        preloaded frame words from raising the register count."""
         m = None
         for m in re.finditer(r"__global__\s+void\s+", head):
             pass
@@ -947,7 +949,7 @@ class Lowering:
                 head = head[:g] + new_defs + head[g:]
             else:
                 tail_defs.append(new_defs)
-            if self.parent:
+            if self.mode == "thread":
                 head = self._bound_kernel(head)
             out.append(head)
             out.append(code)

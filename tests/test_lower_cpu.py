@@ -474,3 +474,34 @@ def test_parent_results_programs_compile(tmp_path, src, defs):
     assert spilled <= 64, lines[k + 1]      # a few registers at most (three queues spill 20 bytes)
     regs = int(re.search(r"Used (\d+) registers", lines[k + 2]).group(1))
     assert regs <= 85, lines[k + 2]
+
+
+@pytest.mark.skipif(shutil.which(NVCC) is None, reason="nvcc not available")
+@pytest.mark.parametrize("src,defs", [
+    ("fib_pragma.cu", "-DGTAP_GRID_SIZE=888 -DGTAP_BLOCK_SIZE=128 -DGTAP_MAX_CHILD_TASKS=2"),
+    ("nq_pragma.cu", "-DGTAP_GRID_SIZE=1184 -DGTAP_BLOCK_SIZE=128 -DGTAP_ASSUME_NO_TASKWAIT"),
+    ("walk_pragma.cu", "-DGTAP_GRID_SIZE=888 -DGTAP_BLOCK_SIZE=128"),
+    ("fib_queues_pragma.cu", "-DGTAP_GRID_SIZE=888 -DGTAP_BLOCK_SIZE=128 -DGTAP_MAX_CHILD_TASKS=2 -DGTAP_NUM_QUEUES=3"),
+    ("bary_tree_pragma.cu", "-DGTAP_GRID_SIZE=888 -DGTAP_BLOCK_SIZE=128 -DGTAP_MAX_CHILD_TASKS=8"),
+])
+def test_default_lowering_keeps_every_worker_resident(tmp_path, src, defs):
+    """The default (retained-result) lowering also bounds the entry kernel:
+    GTAP_GRID_SIZE blocks over 148 SMs must all be resident, so the kernel
+    may use at most 65536 / (threads per SM) registers a thread (1184 x 128
+    threads: 64; 888 x 128: 85)."""
+    out = lower_source(read(src))
+    assert "__launch_bounds__(GTAP_BLOCK_SIZE" in out
+    low = tmp_path / ("retain_" + src)
+    low.write_text(out)
+    cmd = [NVCC, "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-diag-suppress", "550",
+           "-I", os.path.join(ROOT, "include"), "-Xptxas", "-v", "-c", str(low), "-o", str(tmp_path / "prog.o")]
+    r = subprocess.run(cmd + defs.split(), capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-3000:]
+    lines = r.stderr.splitlines()
+    k = next(i for i, ln in enumerate(lines) if "Function properties for _Z11exec_kernel" in ln)
+    regs = int(re.search(r"Used (\d+) registers", lines[k + 2]).group(1))
+    grid = int(re.search(r"GTAP_GRID_SIZE=(\d+)", defs).group(1))
+    threads_per_sm = -(-grid // 148) * 128
+    assert regs * threads_per_sm <= 65536, (regs, threads_per_sm)
+    spilled = int(re.search(r"(\d+) bytes spill stores", lines[k + 1]).group(1))
+    assert spilled <= 64, lines[k + 1]
