@@ -411,8 +411,10 @@ struct BlockProgram {
     }
 };
 
+// 2048 threads per SM at any block size up to kBMaxThreads: at most 32
+// registers a thread, so eight 256-thread workers fit on every SM.
 template <class Prog>
-__global__ void __launch_bounds__(kBMaxThreads) block_worker_kernel(const __grid_constant__ Arena A) {
+__global__ void __launch_bounds__(kBMaxThreads, 2048 / kBMaxThreads) block_worker_kernel(const __grid_constant__ Arena A) {
     __shared__ BlockShared S;
     extern __shared__ __align__(16) int block_smem[];
     block_worker<Prog>(A, S, block_smem);

@@ -72,16 +72,14 @@ struct BlockShared {
 };
 
 // ---------------------------------------------------------------------------
-// single-thread ring pop (the warp version needs all 32 lanes)
+// single-thread pop from the recycled-id pool (the warp version needs all
+// 32 lanes); -1 when the pool is empty
 // ---------------------------------------------------------------------------
-static __device__ int ring_pop_one(const Arena& A, const Ring& r) {
+static __device__ int pool_pop_one(const Arena& A, const Ring& r) {
     const unsigned cap = 1u << r.cap_log2;
     for (int attempt = 0; attempt < 64; ++attempt) {
-        const unsigned h = ld_relaxed(r.head);
-        const unsigned t = ld_relaxed(r.tail);
-        const unsigned avail = t - h;
-        if (avail == 0 || avail > cap) return -1;
-        if (atom_cas_relaxed(r.head, h, h + 1u) == h) {
+        unsigned h = 0;
+        if (pool_claim(r, 1u, h) == 1u) {
             for (int spins = 0; spins <= (1 << 20); ++spins) {
                 const unsigned long long w = ld_acquire(&r.slots[h & (cap - 1)]);
                 if (ring_word_ready(w, h, r.cap_log2)) return ring_word_value(w);
@@ -90,6 +88,8 @@ static __device__ int ring_pop_one(const Arena& A, const Ring& r) {
             GTAP_ERROR(A, ERR_TIMEOUT, -1, -1, (int)h, 0);
             return -1;
         }
+        const unsigned t = ld_relaxed(r.tail), hh = ld_relaxed(r.head);
+        if (t == hh || t - hh > cap) return -1;
     }
     return -1;
 }
@@ -105,7 +105,7 @@ __device__ __forceinline__ const gtap_root& bt_root(const Arena& A, const BlockS
 __device__ __forceinline__ int bt_alloc_id(const Arena& A, BlockShared& S) {
     const int k = atomicSub(&S.avail_n, 1) - 1;
     if (k >= 0) return S.avail[k];
-    const int v = ring_pop_one(A, A.idpool);
+    const int v = pool_pop_one(A, A.idpool);
     if (v >= 0) return v;
     const unsigned f = atomicAdd(A.fresh_next, 1u);
     if (f < (unsigned)A.total_ids) return (int)f;
@@ -435,7 +435,7 @@ static __device__ void bt_refill_ids(const Arena& A, BlockShared& S) {
             if (lane == 0) S.bump += got;
         } else {
             int v = -1;
-            got = ring_pop_warp(A, A.idpool, 32, &v);
+            got = ring_pop_warp(A, A.idpool, 32, &v, true);
             if ((int)lane < got) S.avail[n + lane] = v;
             if (got == 0) {
                 unsigned f = 0;
@@ -541,13 +541,17 @@ static __device__ void bt_round_end(const Arena& A, BlockShared& S) {
             int parent = S.parent;
             bool first = true;
             while (parent >= 0) {
+                // The parent's flags, parent and root are final before any of
+                // its children was published (bt_join writes the header
+                // first), so the header load goes out together with the join
+                // decrement: one round trip per level instead of two.
+                const int4 ph = ld_cg_v4(hdr_of(A, parent));
                 // past the first level this block publishes what it observed
                 // through the previous join (the siblings' data) onwards
                 const int old = first ? atom_add_acquire(&hdr_of(A, parent)->join, -1)
                                       : atom_add_acq_rel(&hdr_of(A, parent)->join, -1);
                 first = false;
                 if ((old & kJoinCountMask) != 1) break;
-                const int4 ph = ld_cg_v4(hdr_of(A, parent));
                 const unsigned pflags = (unsigned)ph.x >> 24;
                 if (!(pflags & kFlagJoinFinish)) {
                     if (next >= 0) {

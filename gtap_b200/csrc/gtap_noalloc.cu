@@ -23,9 +23,10 @@
 //     the free ids each worker keeps at hand; a tree that needs more is
 //     reported as GTAP_ERROR_TASK_ID_POOL_LOW_HEADROOM by the device, not a
 //     fault.  How many tasks are alive at once depends on the tree and the
-//     schedule: a wide tree such as fib(30) without a cutoff, spread over
-//     all workers, exceeds it; trees of up to a few hundred thousand tasks
-//     in all, or with serial cutoffs, fit.
+//     schedule: a tree whose tasks create many children at once, such as
+//     n-queens(16) with every row forking, exceeds it; a binary tree that
+//     waits for its children keeps few alive (fib(34) without a cutoff
+//     fits).
 //
 // Set-up: the first call on a device, with that device current, sizes the
 // grid with an occupancy query.  Make that first call before any stream

@@ -170,10 +170,9 @@ static __device__ __noinline__ int alloc_id_slow(const Arena& A, WarpShared& S) 
     // as the live set requires (rare: the per-round refill keeps the cache full)
     const Ring& r = A.idpool;
     const unsigned cap = 1u << r.cap_log2;
-    for (int attempt = 0; attempt < 4096; ++attempt) {
-        unsigned h = ld_relaxed(r.head), t = ld_relaxed(r.tail);
-        if (t == h || t - h > cap) break;   // pool empty: every id is live
-        if (atom_cas_relaxed(r.head, h, h + 1) == h) {
+    for (int attempt = 0; attempt < 64; ++attempt) {
+        unsigned h = 0;
+        if (pool_claim(r, 1u, h) == 1u) {
             for (int spin = 0; spin < (1 << 20); ++spin) {
                 unsigned long long w = ld_acquire(&r.slots[h & (cap - 1)]);
                 if (ring_word_ready(w, h, r.cap_log2)) return ring_word_value(w);
@@ -182,6 +181,8 @@ static __device__ __noinline__ int alloc_id_slow(const Arena& A, WarpShared& S) 
             GTAP_ERROR(A, ERR_TIMEOUT, -1, -1, (int)h, 0);
             return A.total_ids;
         }
+        const unsigned t = ld_relaxed(r.tail), hh = ld_relaxed(r.head);
+        if (t == hh || t - hh > cap) break;   // pool empty: every id is live
         __nanosleep(32);
     }
     unsigned f = atom_add_relaxed(A.fresh_next, 1u);
@@ -264,7 +265,7 @@ static __device__ void id_cache_maintain(const Arena& A, WarpShared& S) {
         }
         if (got == 0) {
             int id = -1;
-            got = ring_pop_warp(A, A.idpool, 32, &id);
+            got = ring_pop_warp(A, A.idpool, 32, &id, true);
             if ((int)lane < got) S.avail[n + lane] = id;
         }
         if (got == 0) {

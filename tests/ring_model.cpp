@@ -200,6 +200,100 @@ static void replay(uint32_t lg, uint32_t start, uint64_t seed) {
     CHECK(uint32_t(r.tail - start) > 0, "cursor did not move");
 }
 
+// 5. The recycled-id pool's claims (pool_claim in gtap_device.cuh): while
+//    the pool looked long enough, a consumer claims `want` positions with an
+//    add on head instead of a compare-and-swap; positions past the producer
+//    cursor at that moment are given up.  Consumers read (head, tail) in one
+//    step and add in a later one, so other claims interleave and some adds
+//    overshoot (the margin here is small to make that happen).  Checked: no
+//    consumer accepts a word that is not its position's, every produced
+//    value is either accepted once or lies in a given-up position, and no
+//    given-up position is ever read.
+static void pool_claims(uint32_t lg, uint32_t start, uint64_t seed, uint32_t margin) {
+    Ring r(lg);
+    r.head = r.tail = start;
+    std::mt19937_64 rng(seed);
+    const uint32_t cap = 1u << lg;
+    struct Pending { uint32_t pos; int32_t val; };
+    struct Claimer { uint32_t h, t; bool armed; };
+    std::vector<Pending> unwritten;
+    std::vector<uint32_t> claimed;           // positions to read
+    std::vector<Claimer> claimers(16, Claimer{0, 0, false});
+    std::vector<uint8_t> state((size_t)1 << 20, 0);   // by position offset: 1 produced, 2 read, 3 given up
+    std::vector<int32_t> expect((size_t)1 << 20, -1);
+    auto off = [&](uint32_t p) { return (size_t)(uint32_t)(p - start); };
+    int64_t read = 0, given_up = 0, faa = 0;
+    for (int step = 0; step < 40000; ++step) {
+        const int op = (int)(rng() % 4);
+        uint32_t span = r.tail - r.head;
+        for (uint32_t c : claimed) span = std::max(span, r.tail - c);
+        if (op == 0 && span + 32 <= cap && off(r.tail) + 64 < state.size()) {   // push
+            const uint32_t n = 1 + (uint32_t)(rng() % 32);
+            const uint32_t p = r.reserve(n);
+            for (uint32_t i = 0; i < n; ++i) {
+                const int32_t v = (int32_t)(rng() % (1u << 27));
+                unwritten.push_back({p + i, v});
+                expect[off(p + i)] = v;
+            }
+        } else if (op == 1 && !unwritten.empty()) {                              // a producer writes
+            const size_t j = rng() % unwritten.size();
+            r.write(unwritten[j].pos, unwritten[j].val);
+            state[off(unwritten[j].pos)] = state[off(unwritten[j].pos)] == 3 ? 3 : 1;
+            unwritten[j] = unwritten.back();
+            unwritten.pop_back();
+        } else if (op == 2) {                                                    // a claimer acts
+            Claimer& c = claimers[rng() % claimers.size()];
+            const uint32_t want = 1 + (uint32_t)(rng() % 32);
+            if (!c.armed) {                       // first step: read head, then tail
+                c.h = r.head;
+                c.t = r.tail;
+                c.armed = true;
+            } else {                              // second step: claim
+                c.armed = false;
+                const uint32_t avail = c.t - c.h;
+                if (avail == 0 || avail > cap) continue;
+                uint32_t p, got;
+                if (avail >= want + margin) {
+                    p = r.head;
+                    r.head += want;               // the add cannot fail
+                    const int produced = (int)(r.tail - p);
+                    got = produced <= 0 ? 0u : std::min((uint32_t)produced, want);
+                    ++faa;
+                    for (uint32_t i = got; i < want; ++i) {
+                        state[off(p + i)] = 3;
+                        ++given_up;
+                    }
+                } else {
+                    if (r.head != c.h) continue;  // the compare-and-swap fails
+                    got = std::min(avail, want);
+                    p = c.h;
+                    r.head += got;
+                }
+                for (uint32_t i = 0; i < got; ++i) claimed.push_back(p + i);
+            }
+        }
+        for (size_t j = 0; j < claimed.size();) {                                 // claimed positions poll
+            const uint32_t p = claimed[j];
+            CHECK(state[off(p)] != 3, "a given-up position %u was claimed for reading", p);
+            if (r.ready(p)) {
+                CHECK(r.value(p) == expect[off(p)], "position %u read %d, producer wrote %d", p, r.value(p),
+                      expect[off(p)]);
+                CHECK(state[off(p)] == 1, "position %u read before it was written or twice", p);
+                state[off(p)] = 2;
+                ++read;
+                claimed[j] = claimed.back();
+                claimed.pop_back();
+            } else {
+                ++j;
+            }
+        }
+        if (off(r.tail) + 64 >= state.size()) break;
+    }
+    CHECK(read > 1000 && faa > 100, "pool replay exercised too little (read %lld, adds %lld)", (long long)read,
+          (long long)faa);
+    CHECK(given_up > 0, "the small margin should make some adds overshoot");
+}
+
 int main() {
     fresh_ring();
     stale_laps();
@@ -208,6 +302,8 @@ int main() {
     replay(10, 0xFFFFFF00u, 2);
     replay(20, 0xFFFFF000u, 3);
     replay(12, 0, 4);
+    pool_claims(12, 0xFFFFF000u, 5, 8);
+    pool_claims(16, 7, 6, 40);
     if (g_failures) {
         std::printf("%d failures\n", g_failures);
         return 1;

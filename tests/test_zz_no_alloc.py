@@ -134,12 +134,15 @@ def test_noalloc_after_gtap_initialize_with_a_small_block():
 
 def test_noalloc_reports_an_outgrown_scratch_and_recovers():
     """A tree whose live tasks outgrow the 2^19 records of the scratch array
-    (fib(34) without a cutoff, spread over every worker) ends with
-    GTAP_ERROR_TASK_ID_POOL_LOW_HEADROOM, a status the kernel returns, not a
-    fault; the next call starts from a clean scratch and is exact."""
+    ends with GTAP_ERROR_TASK_ID_POOL_LOW_HEADROOM, a status the kernel
+    returns, not a fault; the next call starts from a clean scratch and is
+    exact.  n-queens(16) with every row forking is such a tree: each task
+    creates all of its children at once (up to 16), so some ten rounds of
+    every worker running 32 tasks hold far more than 2^19 ready tasks.
+    (A fib tree keeps its live set small: fib(34) without a cutoff fits.)"""
     import torch
     torch.cuda.init()
-    rc, _ = _noalloc_call([gt.fib_root(34)])
+    rc, _ = _noalloc_call([gt.nq_root(16, 15)])
     assert rc == 6, rc
     _small_roots_exact()
 
