@@ -372,17 +372,22 @@ def main():
         per_root = measure_per_root(gt, roots, res, value / world, overrides)
 
     # serve mode: capacity, then Poisson arrivals at fractions of it and at
-    # 2000 roots/s (the lowest served rate asked for), library defaults
+    # 2000, 5000 and 10000 roots/s (the low end of the served rates asked
+    # for), with the configuration
+    # the autotuner found for the served roots (library defaults without one)
     serve = None
     if args.serve_roots > 0:
         gt.gtap_finalize()
         from gtap_b200 import serve_bench
-        sv = serve_bench.run(loads=(0.5, 0.9), rates=(2000,), count=args.serve_roots)
+        serve_tuned = os.path.join(ROOT, "gtap_b200", "tuned", "b200_serve.json")
+        serve_cfg = load_tuned(serve_tuned)
+        sv = serve_bench.run(loads=(0.5, 0.9), rates=(2000, 5000, 10000), count=args.serve_roots, config=serve_cfg)
         keys = ("load", "rate_roots_per_s", "throughput_roots_per_s", "tasks_per_s", "latency_ms",
                 "device_service_ms", "ok")
         serve = {"workload": "50% async BFS on R-MAT scale 16-20 (edge factor 16), 50% int64 tree sums over "
                              "2^18-2^20-node unbalanced binary trees; Poisson arrivals",
-                 "roots_per_session": args.serve_roots, "config": "library defaults",
+                 "roots_per_session": args.serve_roots,
+                 "config": os.path.relpath(serve_tuned, ROOT) if serve_cfg else "library defaults",
                  "capacity_roots_per_s": sv["capacity"]["throughput_roots_per_s"],
                  "capacity_tasks_per_s": sv["capacity"]["tasks_per_s"],
                  "sessions": [{k: r[k] for k in keys} for r in [sv["capacity"]] + sv["sessions"]],

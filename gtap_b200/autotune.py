@@ -85,10 +85,14 @@ def coordinate_descent(measure, start, space=SPACE, order=ORDER, sweeps=2, log=N
     return best, best_t, trials
 
 
-def _signature(gt, res):
+def _signature(gt, res, kinds=None):
+    """What must not change between configurations: status, value and task
+    count of every root, except the task count of an asynchronous BFS (one
+    task per successful relaxation, which depends on timing)."""
     out = []
-    for r in res:
-        out.append((r.status, r.value, r.tasks))
+    for i, r in enumerate(res):
+        bfs = kinds is not None and kinds[i] == gt.KIND_BFS
+        out.append((r.status, r.value, None if bfs else r.tasks))
     return out
 
 
@@ -100,13 +104,28 @@ def run(workload="mix", reps=3, sweeps=2, n_roots=None, out=None, quiet=False, s
     torch.cuda.init()
     sm_count = torch.cuda.get_device_properties(0).multi_processor_count
     keep = []
+    before = None   # runs before every launch (resets what a launch consumes)
     if workload == "mix":
         mix = wl.Mix(gt, n_roots or wl.N_ROOTS)
         src, arr, tmp = mix.device_slabs()
         keep += [src, arr, tmp]
         roots = mix.roots(gt, src.data_ptr(), arr.data_ptr(), tmp.data_ptr())
+    elif workload == "serve":
+        # the served workload's roots (BFS on R-MAT 16-20, tree sums of
+        # 2^18-2^20 nodes) in one batch launch of the kernel serve mode runs:
+        # the session's capacity when every root is enqueued at once
+        from gtap_b200.serve_bench import ServeWorkload
+        sw = ServeWorkload(gt)
+        roots, depths = sw.roots(sw.draw(n_roots or 200))
+        keep += [sw, depths]
+
+        def before():
+            for d in depths:
+                if d is not None:
+                    d.fill_(0x3f3f3f3f)
     else:
         roots = wl.single_root_workload(gt, workload)
+    kinds = [r.kind for r in roots]
     # every kind in these workloads has a fixed task tree (cilksort's depends
     # only on the keys), so values and task counts must not change
     ref_sig = {}
@@ -118,14 +137,18 @@ def run(workload="mix", reps=3, sweeps=2, n_roots=None, out=None, quiet=False, s
         except gt.GtapError:
             return None
         try:
+            if before:
+                before()
             res, st = gt.launch(roots)                      # warm-up
-            sig = _signature(gt, res)
+            sig = _signature(gt, res, kinds)
             if "sig" not in ref_sig:
                 ref_sig["sig"] = sig
             elif sig != ref_sig["sig"]:
                 raise RuntimeError("configuration %s changed a result" % over)
             ms = []
             for _ in range(reps):
+                if before:
+                    before()
                 res, st = gt.launch(roots)
                 ms.append(st.kernel_ms)
             return statistics.median(ms) / 1e3
@@ -169,7 +192,7 @@ def load_tuned(path):
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    ap.add_argument("--workload", default="mix", choices=["mix", "fib30", "fib34c12", "nq13", "nq13c7"])
+    ap.add_argument("--workload", default="mix", choices=["mix", "serve", "fib30", "fib34c12", "nq13", "nq13c7"])
     ap.add_argument("--roots", type=int, default=None)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--sweeps", type=int, default=2)
