@@ -21,6 +21,13 @@ first trial's (values, task counts of deterministic kinds, statuses), so a
 configuration that breaks a result cannot win.
 
     python -m gtap_b200.autotune --workload mix --out gtap_b200/tuned/b200_mix.json
+    python -m gtap_b200.autotune --workload serve --out gtap_b200/tuned/b200_serve.json
+
+The serve workload is the served roots (BFS on R-MAT 16-20, tree sums of
+2^18-2^20 nodes, 200 of them) in one batch launch of the kernel serve mode
+runs, the session's capacity when every root arrives at once; BFS depth arrays
+are reset before every launch, and a BFS root's task count (timing-dependent)
+is left out of the result check.
 """
 import argparse
 import json
