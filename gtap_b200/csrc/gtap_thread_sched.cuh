@@ -1031,50 +1031,32 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
         const unsigned fin = __ballot_sync(0xffffffffu, active && (lane_flags & kLaneFinished));
         const bool my_fin = active && ((fin >> lane) & 1u);
         const unsigned spawners = __ballot_sync(0xffffffffu, active && S.l_spawned[lane] > 0);
-        // (0) root accounting, once per round and one leader per distinct
-        //     root: the children this round created count for their roots
-        //     before any of them can be seen by another warp (one that ran
-        //     and finished elsewhere before its creation was counted could
-        //     bring its root's counter to zero early); the round's finishes
-        //     and values are booked in the same call, values first.  Booking
-        //     a finish before the join decrement in (3) cannot complete a root
-        //     early: the parent it resumes is still counted.
+        // (0) the children this round created count for their roots before
+        //     any of them can be seen by another warp: one that ran and
+        //     finished elsewhere before its creation was counted could bring
+        //     its root's counter to zero early.  One leader per distinct root.
         const int r0 = S.l_root[0];   // lane 0 always runs a task when nb > 0
         const bool one_root = __all_sync(0xffffffffu, !active || S.l_root[lane] == r0);
         const int my_root = active ? S.l_root[lane] : -1;
         const unsigned grp = one_root ? 0xffffffffu : __match_any_sync(0xffffffffu, my_root);
         {
             const int created = active ? S.l_created[lane] : 0;
-            if (one_root) {
-                const int c_sum = (int)__reduce_add_sync(0xffffffffu, (unsigned)created);
-                const int v_sum = (int)__reduce_add_sync(0xffffffffu, active ? (unsigned)S.l_value[lane] : 0u);
-                if (lane == 0) {
-                    if (v_sum) atomicAdd(reinterpret_cast<unsigned long long*>(&A.results[r0].value),
-                                         (unsigned long long)(long long)v_sum);
-                    account_root(A, S, r0, c_sum, __popc(fin));
-                    if (S.nbal > 1) age_bal(A, S);
-                    else S.bal[0].touched = 0;
-                }
-            } else {
-                int c_sum = 0, v_sum = 0, f_sum = 0;
-                if (active) {
-                    c_sum = (int)__reduce_add_sync(grp, (unsigned)created);
-                    v_sum = (int)__reduce_add_sync(grp, (unsigned)S.l_value[lane]);
-                    f_sum = __popc(fin & grp);
-                }
-                unsigned leaders = __ballot_sync(0xffffffffu, active && (unsigned)__ffs(grp) - 1u == lane);
-                while (leaders) {
-                    if (lane == (unsigned)__ffs(leaders) - 1u) {
-                        if (v_sum) atomicAdd(reinterpret_cast<unsigned long long*>(&A.results[my_root].value),
-                                             (unsigned long long)(long long)v_sum);
-                        account_root(A, S, my_root, c_sum, f_sum);
+            if (__any_sync(0xffffffffu, created != 0)) {
+                if (one_root) {
+                    const int c_sum = (int)__reduce_add_sync(0xffffffffu, (unsigned)created);
+                    if (lane == 0) account_root(A, S, r0, c_sum, 0);
+                } else {
+                    int c_sum = 0;
+                    if (active) c_sum = (int)__reduce_add_sync(grp, (unsigned)created);
+                    unsigned leaders = __ballot_sync(0xffffffffu, active && c_sum != 0 && (unsigned)__ffs(grp) - 1u == lane);
+                    while (leaders) {
+                        if (lane == (unsigned)__ffs(leaders) - 1u) account_root(A, S, my_root, c_sum, 0);
+                        __syncwarp();
+                        leaders &= leaders - 1u;
                     }
-                    __syncwarp();
-                    leaders &= leaders - 1u;
                 }
-                if (lane == 0) age_bal(A, S);
+                __syncwarp();
             }
-            __syncwarp();
         }
         //     Detached children that did not fit the staging buffer and still
         //     wait (one per lane, charged when spawned): their frames are
@@ -1230,6 +1212,44 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
         publish_commit(A, S, P, false);
         GTAP_PHASE_MARK(ph4);
         GTAP_PHASE_ADD(13, ph3b, ph4);
+        // (6) per-root accounting of finishes and values (creations were
+        //     charged in (0)), one leader per distinct root
+        if (one_root) {
+            // every task of the round belongs to one root: warp sums, lane 0 books them
+            const unsigned value = active ? (unsigned)S.l_value[lane] : 0u;
+            const int f_sum = __popc(fin);
+            const int v_sum = (int)__reduce_add_sync(0xffffffffu, value);
+            if (lane == 0) {
+                if (v_sum) atomicAdd(reinterpret_cast<unsigned long long*>(&A.results[r0].value),
+                                     (unsigned long long)(long long)v_sum);
+                account_root(A, S, r0, 0, f_sum);
+                if (S.nbal > 1) age_bal(A, S);
+                else S.bal[0].touched = 0;
+            }
+            __syncwarp();
+        } else {
+            const int value = active ? S.l_value[lane] : 0;
+            int f_sum = 0, v_sum = 0;
+            if (active) {
+                f_sum = __popc(fin & grp);
+                v_sum = (int)__reduce_add_sync(grp, (unsigned)value);
+            }
+            const bool leader = active && ((unsigned)__ffs(grp) - 1u == lane);
+            unsigned leaders = __ballot_sync(0xffffffffu, leader);
+            __syncwarp();
+            while (leaders) {
+                const unsigned l = (unsigned)__ffs(leaders) - 1u;
+                if (lane == l) {
+                    if (v_sum) atomicAdd(reinterpret_cast<unsigned long long*>(&A.results[my_root].value),
+                                         (unsigned long long)(long long)v_sum);
+                    account_root(A, S, my_root, 0, f_sum);
+                }
+                __syncwarp();
+                leaders &= leaders - 1u;
+            }
+            if (lane == 0) age_bal(A, S);
+            __syncwarp();
+        }
         __syncwarp();
         if (lane == 0) {
             for (int k = 0; k < A.num_queues; ++k) S.cnt[k] = 0;
