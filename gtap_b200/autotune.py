@@ -14,6 +14,8 @@ Search: coordinate descent from the library defaults over
   probe_width    victims probed in parallel per steal attempt
   victim_policy  random / last success / fullest of the probed
   num_queues     EPAQ queues
+  spawn_capacity children staged per worker and round (shared memory per warp,
+                 so it also sets how many workers fit an SM)
 Each trial re-initialises the runtime with the candidate configuration, runs
 one warm-up launch and `reps` timed launches (CUDA events around the
 persistent kernel) and keeps the median.  Every trial's results must equal the
@@ -44,8 +46,10 @@ SPACE = {
     "probe_width": [1, 4, 16, 32],
     "victim_policy": [0, 1, 2],
     "num_queues": [1, 2, 4],
+    "spawn_capacity": [128, 256, 512, 1024],
 }
-ORDER = ["warps_per_sm", "block", "steal_batch", "deque_capacity", "probe_width", "victim_policy", "num_queues"]
+ORDER = ["warps_per_sm", "block", "steal_batch", "deque_capacity", "probe_width", "victim_policy", "num_queues",
+         "spawn_capacity"]
 
 
 def to_overrides(point, sm_count):
@@ -171,7 +175,8 @@ def run(workload="mix", reps=3, sweeps=2, n_roots=None, out=None, quiet=False, s
     defaults = gt.default_config()
     start = {"warps_per_sm": 8, "block": defaults.block, "deque_capacity": defaults.deque_capacity,
              "steal_batch": defaults.steal_batch, "probe_width": defaults.probe_width,
-             "victim_policy": defaults.victim_policy, "num_queues": defaults.num_queues}
+             "victim_policy": defaults.victim_policy, "num_queues": defaults.num_queues,
+             "spawn_capacity": defaults.spawn_capacity}
     start.update(start_point or {})
     t0 = time.time()
     best, best_t, trials = coordinate_descent(measure, start, sweeps=sweeps, log=log)

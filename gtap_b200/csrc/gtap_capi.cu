@@ -495,7 +495,8 @@ static int initialize_impl(const gtap_config* cfg_in, int external_workers) {
     int per_sm_full = 0, per_sm_light = 0;
     GT_CUDA(cudaFuncSetAttribute(kernel_full(c.num_queues), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_full));
     GT_CUDA(cudaFuncSetAttribute(kernel_light(c.num_queues), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    GT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_full, kernel_full(c.num_queues), c.block, smem_full));
+    if (c.block <= kFullKernelThreads)   // the sorting kernel's launch bound
+        GT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_full, kernel_full(c.num_queues), c.block, smem_full));
     GT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_light, kernel_light(c.num_queues), c.block, smem));
     if (per_sm_light < 1) return GTAP_ERROR_INVALID_ARGUMENT;
     // one resident wave per variant; grid = 0 fills the GPU, otherwise cap it

@@ -1344,8 +1344,13 @@ __device__ __forceinline__ void thread_worker_body(const Arena& A) {
 // __grid_constant__ lets the scheduler take its address without the compiler
 // copying its 400-odd bytes into every thread's local memory, where each field
 // read would be a local load that mostly misses L1.
+// At most kFullKernelThreads threads per block and 72 registers a thread:
+// with 128-thread blocks seven workers' blocks fit an SM by registers (88
+// unbounded registers allowed five), which runs the mix's fib and n-queens
+// tasks faster than the few spills cost the sort paths.
+constexpr int kFullKernelThreads = 896;
 template <class Prog, int QM>
-__global__ void thread_worker_kernel(const __grid_constant__ Arena A) {
+__global__ void __launch_bounds__(kFullKernelThreads, 1) thread_worker_kernel(const __grid_constant__ Arena A) {
     thread_worker_body<Prog, QM>(A);
 }
 
