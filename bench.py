@@ -408,11 +408,13 @@ def main():
         msort = measure_mergesort_thread(gt, args.mergesort_keys, args.steps, args.warmup, hbm_peak=hbm,
                                          overrides=json.loads(args.config) if args.config else {})
 
-    # the reference GTaP GPU build on fib, beside this runtime (same box, same call)
+    # the reference GTaP GPU build on fib, beside this runtime (same box, same call),
+    # and as the per-root baseline for the mix's fib roots
     ref_gpu = None
     if args.reference_gpu and rank == 0:
         gt.gtap_finalize()
         ref_gpu = measure_reference_gpu(gt)
+        ref_gpu["per_root_fib_roots_of_the_mix"] = measure_reference_per_root(gt, mix, overrides)
 
     published = single = None
     if args.extras and rank == 0:
@@ -778,6 +780,47 @@ def measure_single_roots(gt, reps=3):
     finally:
         gt.gtap_finalize()
     return out
+
+
+def measure_reference_per_root(gt, mix, overrides, reps=6):
+    """The plain per-root baseline with the reference GTaP build itself, for
+    the mix's fib roots (the reference build of fib is the one that runs
+    correctly here): each distinct n timed by oracle/_ref/fib_ref (the
+    reference runtime, gtap_reset + one launch per run, CUDA events around
+    the launch, so the reset is not even counted), times the number of roots
+    with that n; against the same fib roots batched in one launch of this
+    runtime with the mix's configuration."""
+    import subprocess as sp
+    from tests import oracle_lib as orc
+    exe = os.path.join(ROOT, "oracle", "_ref", "fib_ref")
+    if not os.path.exists(exe):
+        return {"note": "oracle/_ref/fib_ref not built (oracle/Makefile ref-gpu needs the reference sources)"}
+    fib_idx = [i for i in range(mix.n) if int(mix.kind[i]) == 0]
+    ns = sorted({int(mix.param[i]) for i in fib_idx})
+    per_n = {}
+    for n in ns:
+        r = sp.run([exe, str(n), "0", str(reps)], capture_output=True, text=True, timeout=120)
+        d = json.loads(r.stdout.strip().splitlines()[-1])
+        if r.returncode != 0 or d.get("result") != orc.fib(n):
+            return {"note": "reference build failed on fib(%d)" % n}
+        per_n[n] = statistics.median(d["ms"][1:])
+    ref_ms = sum(per_n[int(mix.param[i])] for i in fib_idx)
+    tasks = sum(orc.fib_tasks(int(mix.param[i]), 0) for i in fib_idx)
+    roots = [gt.fib_root(int(mix.param[i]), 0) for i in fib_idx]
+    gt.gtap_initialize(gt.default_config(**overrides))
+    try:
+        ms = []
+        for _ in range(4):
+            res, st = gt.launch(roots)
+            assert all(r.value == orc.fib(int(mix.param[i])) for r, i in zip(res, fib_idx))
+            ms.append(st.kernel_ms)
+    finally:
+        gt.gtap_finalize()
+    ours = statistics.median(ms[1:])
+    return {"roots": len(fib_idx), "tasks": tasks, "reference_build_per_root_ms": ref_ms,
+            "reference_build_tasks_per_s": tasks / (ref_ms / 1e3), "batched_ms": ours,
+            "batched_tasks_per_s": tasks / (ours / 1e3), "speedup_batched_vs_reference_per_root": ref_ms / ours,
+            "per_n_ms": per_n}
 
 
 def atomic_view(counters, mix, res, k_ms):
