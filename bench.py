@@ -70,28 +70,55 @@ def parse():
 
 
 def algorithmic_bytes(mix, results):
-    """Bytes per step the algorithm must move.  fib tasks: the parent's argument
-    write and the child's read of a frame, the deque slot write and read, the
-    join-counter update and the result read.  n-queens tasks (no join): the
-    frame write and read and the deque slot.  cilksort roots: each task's
-    frame, deque slot and join counter, plus 8 bytes per key (a 4-byte read
-    and write) for the leaf pass and for two merge passes per four-way level."""
-    total = 0
+    """Bytes per step the algorithm must move, as (fib and n-queens roots,
+    cilksort roots).  fib tasks: the parent's argument write and the child's
+    read of a frame, the deque slot write and read, the join-counter update and
+    the result read.  n-queens tasks (no join): the frame write and read and
+    the deque slot.  cilksort roots: each task's frame, deque slot and join
+    counter, plus 8 bytes per key (a 4-byte read and write) for the leaf pass
+    and for two merge passes per four-way level."""
+    light = sort = 0
     for i, r in enumerate(results):
         k = int(mix.kind[i])
         if k == 0:
-            total += r.tasks * (2 * S_FIB + 8 + 8 + 4)
+            light += r.tasks * (2 * S_FIB + 8 + 8 + 4)
         elif k == 1:
-            total += r.tasks * (2 * S_NQ + 8)
+            light += r.tasks * (2 * S_NQ + 8)
         else:
             n = int(mix.param[i])
             levels, m = 0, n
             while m >= SORT_CUTOFF:
                 m //= 4
                 levels += 1
-            total += r.tasks * (2 * S_MERGE + 8 + 8)     # task overhead
-            total += n * 8 * (1 + 2 * levels)             # leaf pass + two merge passes per level
-    return total
+            sort += r.tasks * (2 * S_MERGE + 8 + 8)     # task overhead
+            sort += n * 8 * (1 + 2 * levels)             # leaf pass + two merge passes per level
+    return light, sort
+
+
+LIGHT_KERNEL = "gtap::thread_worker_kernel_lb<BuiltinProgramLight>"
+FULL_KERNEL = "gtap::thread_worker_kernel<BuiltinProgram>"
+
+
+def worker_kernels(alg_light, alg_sort, light_ms, full_ms, hbm):
+    """Per worker kernel of a step: its roots, mean launch time, algorithmic
+    bytes and the fraction of the measured copy bandwidth they come to.  A
+    split batch runs the fib and n-queens roots in the kernel without sort
+    leaves and the cilksort roots in the sort-capable one; an unsplit batch
+    runs all of them in the sort-capable kernel."""
+    out = []
+    if light_ms > 0:
+        out.append({"kernel": LIGHT_KERNEL, "roots": "fib and n-queens", "ms": light_ms,
+                    "algorithmic_bytes": alg_light, "traffic": scaled_traffic("light_kernel", alg_light)})
+        if full_ms > 0:
+            out.append({"kernel": FULL_KERNEL, "roots": "cilksort", "ms": full_ms, "algorithmic_bytes": alg_sort,
+                        "traffic": scaled_traffic("sort_kernel", alg_sort)})
+    else:
+        out.append({"kernel": FULL_KERNEL, "roots": "all", "ms": full_ms, "algorithmic_bytes": alg_light + alg_sort,
+                    "traffic": scaled_traffic("mixed_kernel", alg_light + alg_sort)})
+    for k in out:
+        k["achieved_gbs"] = k["algorithmic_bytes"] / (k["ms"] / 1e3) / 1e9
+        k["frac"] = k["achieved_gbs"] / hbm
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -324,9 +351,11 @@ def main():
     e1 = torch.cuda.Event(enable_timing=True)
     kern_ms, tasks_step, stats_acc = [], [], None
     e0.record()
+    light_ms = []
     for _ in range(args.steps):
         res, st = gt.launch(roots)
         kern_ms.append(st.kernel_ms)
+        light_ms.append(st.light_kernel_ms)
         tasks_step.append(sum(r.tasks for r in res))
         stats_acc = st
     e1.record()
@@ -340,9 +369,10 @@ def main():
     # the last timed launch's results must be the verified ones
     verified = verified and all(r.status == gt.ROOT_DONE for r in res) and tasks_per_step == tasks_step[0]
 
-    # roofline: dominant kernel = the persistent worker
-    alg_bytes = algorithmic_bytes(mix, res)
+    # roofline: the dominant kernel = the worker kernel with the larger share of the step
+    alg_light, alg_sort = algorithmic_bytes(mix, res)
     k_ms = statistics.mean(kern_ms)
+    l_ms = statistics.mean(light_ms)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -351,13 +381,13 @@ def main():
     hbm = peaks.get("hbm_gbs")
     peak_src = "measured" if hbm else "fallback"
     hbm = hbm or 6650.0
-    achieved = alg_bytes / (k_ms / 1e3) / 1e9
+    kernels = worker_kernels(alg_light, alg_sort, l_ms, k_ms - l_ms, hbm)
+    top = max(kernels, key=lambda k: k["ms"])
     counters = stats_acc.as_dict() if stats_acc else {}
-    roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-            "traffic": traffic_from_profile(), "peak_source": peak_src,
-            "kernel": "gtap::thread_worker_kernel<BuiltinProgram>", "kernel_ms": k_ms,
-            "algorithmic_bytes_per_launch": alg_bytes,
-            "atomic": atomic_view(counters, mix, res, k_ms)}
+    roof = {"bound": "hbm", "achieved": top["achieved_gbs"], "peak": hbm, "unit": "GB/s", "frac": top["frac"],
+            "traffic": top["traffic"], "peak_source": peak_src, "kernel": top["kernel"], "kernel_ms": top["ms"],
+            "algorithmic_bytes_per_launch": top["algorithmic_bytes"], "worker_kernels": kernels,
+            "worker_ms_per_step": k_ms, "atomic": atomic_view(counters, mix, res, k_ms)}
 
     # e2e through the host-buffer entry point (H2D keys, D2H sorted keys + results)
     e2e = None
@@ -435,8 +465,9 @@ def main():
 
     W = int(counters.get("workers", 0))
     sched = {"steal_success_rate": counters.get("steal_successes", 0) / max(1, counters.get("steal_attempts", 0)),
-             "idle_worker_fraction": counters.get("idle_ns", 0) / max(1.0, W * kern_ms[-1] * 1e6),
-             "workers": W, "idle_polls": counters.get("idle_polls", 0),
+             "idle_worker_fraction": counters.get("idle_ns", 0) / max(1.0, stats_acc.worker_ms() * 1e6),
+             "workers": W, "light_workers": int(counters.get("light_workers", 0)),
+             "launches_per_step": int(counters.get("launches", 1)), "idle_polls": counters.get("idle_polls", 0),
              "executions": counters.get("executions", 0), "rounds": counters.get("rounds", 0),
              "tasks_per_round": counters.get("executions", 0) / max(1, counters.get("rounds", 0))}
     # order: the contract's keys first, the large per-mode objects next, the
@@ -447,7 +478,7 @@ def main():
             "config": workload_config(mix), "tasks_per_step": tasks_per_step,
             "parallelism": "replicas" if world > 1 else "single GPU",
             "runtime": {"config": cfg.as_dict(), "tuned_from": tuned_from},
-            "verified": verified, "gpu_launches": 2 * args.steps, "e2e": e2e, "roofline": roof,
+            "verified": verified, "gpu_launches": 2 * int(counters.get("launches", 1)) * args.steps, "e2e": e2e, "roofline": roof,
             "cpu_baseline": cpu, "clocks": ck, "serve": serve, "block_mode": block, "mergesort_thread": msort,
             "single_roots": single, "published_configs": published,
             "reference_gpu": ref_gpu, "per_root_launch": per_root, "scheduler": sched}
@@ -880,13 +911,21 @@ def measure_e2e(gt, mix, steps, tasks_per_step, world, arr_dev):
             "ok": ok}
 
 
-def traffic_from_profile(key="worker_kernel_dram_bytes_per_launch"):
+def traffic_from_profile(key):
     """A figure from the committed ncu summary of DRAM traffic, if any."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         return json.load(open(p)).get(key)
     except Exception:
         return None
+
+
+def scaled_traffic(kernel, alg_bytes):
+    """DRAM bytes per launch of a worker kernel: the traffic / algorithmic-bytes
+    ratio ncu measured for it on a smaller case of the same roots, times this
+    launch's algorithmic bytes (null without a committed measurement)."""
+    r = traffic_from_profile(kernel + "_traffic_over_algorithmic")
+    return None if r is None else int(alg_bytes * r)
 
 
 if __name__ == "__main__":

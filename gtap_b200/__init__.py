@@ -26,6 +26,7 @@ elif os.environ.get("GTAP_LIB_VARIANT") == "debug":
 # ---- constants mirrored from include/gtap.h --------------------------------
 MODE_THREAD, MODE_BLOCK = 0, 1
 VICTIM_RANDOM, VICTIM_LAST_SUCCESS, VICTIM_PROBE_MAX = 0, 1, 2
+ADMIT_AS_GIVEN, ADMIT_BY_KIND, ADMIT_SPLIT = 0, 1, 2
 KIND_FIB, KIND_NQ, KIND_CILKSORT, KIND_MERGESORT, KIND_BFS, KIND_TREESUM = 1, 2, 3, 4, 5, 6
 ROOT_PENDING, ROOT_RUNNING, ROOT_DONE = 0, 1, 2
 
@@ -53,6 +54,7 @@ class Config(ctypes.Structure):
         ("ids_per_worker", ctypes.c_int32), ("total_ids", ctypes.c_int64), ("frame_bytes", ctypes.c_int32),
         ("admit_batch", ctypes.c_int32), ("watchdog_ms", ctypes.c_int64), ("profile_samples", ctypes.c_int32),
         ("result_handles", ctypes.c_int32), ("publish_lazy", ctypes.c_int32), ("max_inflight_roots", ctypes.c_int32),
+        ("admit_order", ctypes.c_int32),
     ]
 
     def as_dict(self):
@@ -78,13 +80,21 @@ class RunStats(ctypes.Structure):
     _fields_ = [
         ("counters", ctypes.c_uint64 * STAT_COUNT), ("kernel_ms", ctypes.c_double), ("grid", ctypes.c_int32),
         ("block", ctypes.c_int32), ("workers", ctypes.c_int32), ("status", ctypes.c_int32),
+        ("launches", ctypes.c_int32), ("light_workers", ctypes.c_int32), ("light_kernel_ms", ctypes.c_double),
     ]
 
     def as_dict(self):
         d = {name: int(self.counters[i]) for i, name in enumerate(STAT_NAMES)}
         d.update(kernel_ms=self.kernel_ms, grid=self.grid, block=self.block, workers=self.workers,
-                 status=self.status)
+                 status=self.status, launches=self.launches, light_workers=self.light_workers,
+                 light_kernel_ms=self.light_kernel_ms)
         return d
+
+    def worker_ms(self):
+        """Workers x milliseconds over the launches (the idle fraction's denominator)."""
+        full_ms = self.kernel_ms - self.light_kernel_ms
+        full_workers = self.workers if full_ms > 0 else 0
+        return self.light_workers * self.light_kernel_ms + full_workers * full_ms
 
 
 class ErrorReport(ctypes.Structure):
@@ -132,6 +142,7 @@ _SIGS = [
      [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32] + [ctypes.POINTER(ctypes.c_int64)] * 4),
     ("gtap_get_arena_counters", ctypes.c_int, [ctypes.POINTER(ctypes.c_int64), ctypes.c_int32]),
     ("gtap_debug_set_ring_position", ctypes.c_int, [ctypes.c_int32, ctypes.c_uint32]),
+    ("gtap_debug_admission_order", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]),
     ("gtap_measure_atomic_rate", ctypes.c_int, [ctypes.c_int32, ctypes.c_int64, ctypes.POINTER(ctypes.c_double)]),
     ("gtap_launch_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]),
     # support of the drop-in task-ABI header for caller-launched kernels
@@ -338,6 +349,16 @@ def set_ring_position(position, target=0):
     """Testing aid: both global rings empty, cursors at `position` (0..2^32-1).
     target 0 = the gtap_initialize arena, 1 = gtap_launch_noalloc's scratch."""
     _check(lib().gtap_debug_set_ring_position(target, position & 0xFFFFFFFF), "gtap_debug_set_ring_position")
+
+
+def admission_order(roots):
+    """(order, n_light): the order a grouped batch launch admits roots in (host only)."""
+    arr = _root_array(roots)
+    order = (ctypes.c_int32 * max(1, len(roots)))()
+    n_light = ctypes.c_int32(0)
+    _check(lib().gtap_debug_admission_order(arr, len(roots), order, ctypes.byref(n_light)),
+           "gtap_debug_admission_order")
+    return [order[i] for i in range(len(roots))], n_light.value
 
 
 def measure_atomic_rate(mode=0, ops=1 << 28):

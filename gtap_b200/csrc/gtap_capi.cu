@@ -11,9 +11,11 @@
 #include <algorithm>
 #include <cerrno>
 #include <climits>
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <mutex>
 #include <random>
 #include <string>
@@ -153,6 +155,60 @@ bool roots_need_sorts(const gtap_root* roots, int n) {
     return false;
 }
 
+// layouts the Python binding and other FFI callers mirror
+static_assert(sizeof(gtap_config) == 88 && offsetof(gtap_config, admit_order) == 80, "gtap_config layout");
+static_assert(sizeof(gtap_run_stats) == 168 && offsetof(gtap_run_stats, light_kernel_ms) == 160,
+              "gtap_run_stats layout");
+static_assert(sizeof(gtap_root) == 56 && sizeof(gtap_root_result) == 40, "root layouts");
+
+bool is_sort_kind(int kind) { return kind == GTAP_KIND_CILKSORT || kind == GTAP_KIND_MERGESORT; }
+
+// Frame bytes the tasks of a root kind use at most: fib, n-queens and BFS
+// tasks keep 16-byte frames, so a launch of those alone packs a task record
+// (16-byte header + frame) into one 32-byte sector instead of 48 bytes.
+static_assert(sizeof(prog::FibFrame) <= 16 && sizeof(prog::NqFrame) <= 16 && sizeof(prog::BfsFrame) <= 16,
+              "16-byte frames");
+int frame_bytes_of(int kind) {
+    return (kind == GTAP_KIND_FIB || kind == GTAP_KIND_NQ || kind == GTAP_KIND_BFS) ? 16 : BuiltinProgram::kFrameBytes;
+}
+
+// Record stride of a launch over roots[0, n): the configured one, or less
+// when every kind of those roots needs less.
+int record_stride_for(const gtap_root* roots, int n) {
+    int need = 16;
+    for (int i = 0; i < n && need < BuiltinProgram::kFrameBytes; ++i) need = std::max(need, frame_bytes_of(roots[i].kind));
+    const int configured = kHdrBytes + ((g.cfg.frame_bytes + 15) / 16) * 16;
+    return std::min(configured, kHdrBytes + ((need + 15) / 16) * 16);
+}
+
+// Stable grouping of a batch by kind: the kinds without sort leaves first (in
+// kind order), then the sorts; kinds out of range lead, so that their error
+// is raised before any other root runs.  Fills order (slot -> caller index)
+// unless the batch is grouped already, and returns the number of roots ahead
+// of the first sort.
+int admission_order(const gtap_root* roots, int n, std::vector<int>& order) {
+    auto group = [](int kind) {
+        if (kind < GTAP_KIND_FIB || kind >= GTAP_KIND_COUNT) return 0;
+        return is_sort_kind(kind) ? GTAP_KIND_COUNT + kind : kind;
+    };
+    constexpr int kGroups = 2 * GTAP_KIND_COUNT;
+    int count[kGroups + 1] = {0};
+    bool grouped = true;
+    int prev = 0;
+    for (int i = 0; i < n; ++i) {
+        const int k = group(roots[i].kind);
+        count[k + 1]++;
+        if (k < prev) grouped = false;
+        prev = k;
+    }
+    for (int k = 0; k < kGroups; ++k) count[k + 1] += count[k];
+    const int n_light = count[GTAP_KIND_COUNT + 1];
+    if (grouped) return n_light;
+    order.resize(n);
+    for (int i = 0; i < n; ++i) order[count[group(roots[i].kind)]++] = i;
+    return n_light;
+}
+
 constexpr size_t kBlockSmemBytes = (size_t)BlockProgram::kSmemInts * sizeof(int);
 
 bool block_mode() { return g.cfg.mode == GTAP_MODE_BLOCK; }
@@ -215,7 +271,8 @@ __global__ void reset_kernel(Arena A, unsigned* counters, int n_roots, int fresh
     }
 }
 
-Arena make_arena(int n_roots, int mode, int workers) {
+// first_root: the batch's roots, results and balances start at this slot
+Arena make_arena(int n_roots, int mode, int workers, int first_root = 0) {
     Arena A{};
     const gtap_config& c = g.cfg;
     A.num_workers = workers;
@@ -248,9 +305,9 @@ Arena make_arena(int n_roots, int mode, int workers) {
     A.idpool.tail = g.counters + kCtrPoolTail;
     A.idpool.cap_log2 = g.idpool_log2;
     A.fresh_next = g.counters + kCtrFresh;
-    A.roots = g.d_roots;
-    A.results = g.d_results;
-    A.outstanding = g.d_outstanding;
+    A.roots = g.d_roots + first_root;
+    A.results = g.d_results + first_root;
+    A.outstanding = g.d_outstanding + first_root;
     A.n_roots = n_roots;
     A.next_root = g.counters + kCtrNextRoot;
     A.published = g.counters + kCtrPublished;
@@ -317,6 +374,7 @@ int validate_config(const gtap_config& c) {
     if (c.watchdog_ms < 1) return GTAP_ERROR_INVALID_ARGUMENT;
     if (c.profile_samples < 0 || c.result_handles < 1) return GTAP_ERROR_INVALID_ARGUMENT;
     if (c.publish_lazy < 0 || c.publish_lazy > 1 || c.max_inflight_roots < 0) return GTAP_ERROR_INVALID_ARGUMENT;
+    if (c.admit_order < GTAP_ADMIT_AS_GIVEN || c.admit_order > GTAP_ADMIT_SPLIT) return GTAP_ERROR_INVALID_ARGUMENT;
     return 0;
 }
 
@@ -375,8 +433,9 @@ int collect_stats(gtap_run_stats* stats) {
     return 0;
 }
 
-// One persistent launch over roots already in g.d_roots.
-int launch_resident(int n_roots, cudaStream_t s, float* ms_out, bool light) {
+// One persistent launch over the roots already in g.d_roots[first_root, first_root + n_roots).
+// rec_stride > 0: the record stride of this launch (at most the configured one).
+int launch_resident(int n_roots, cudaStream_t s, float* ms_out, bool light, int first_root = 0, int rec_stride = 0) {
     if (g.cfg.profile_samples > 0) {
         size_t n = (size_t)g.workers * g.cfg.profile_samples;
         GT_CUDA(cudaMemsetAsync(g.prof_having, 0, n * sizeof(long long), s));
@@ -391,7 +450,8 @@ int launch_resident(int n_roots, cudaStream_t s, float* ms_out, bool light) {
     const int W = block_mode() ? g.workers_block : light ? g.workers_light : g.workers_full;
     g.last_workers = W;
     g.last_block = block_mode();
-    Arena A = make_arena(n_roots, 0, W);
+    Arena A = make_arena(n_roots, 0, W, first_root);
+    if (rec_stride > 0 && rec_stride < A.rec_stride) A.rec_stride = rec_stride;
     const int fresh_base = W * g.cfg.ids_per_worker;
     A.admit_watermark = admission_watermark(W);
     reset_kernel<<<std::max(1, std::min(1184, (std::max(n_roots, W * g.cfg.num_queues) + 255) / 256)), 256, 0,
@@ -430,6 +490,143 @@ __global__ void external_root_kernel(Arena A, unsigned* counters) {
     counters[kCtrNextRoot] = 1;   // nothing left to admit
 }
 
+
+// Hooks of a host-buffer batch (gtap_run_host): the sort roots' inputs arrive
+// on another stream while a launch without sorts runs, and their outputs leave
+// while the last launch runs.
+struct BatchHooks {
+    std::function<int()> before_launches;   // issues the input copies, after the root table's copy
+    cudaEvent_t sort_inputs = nullptr;   // recorded after the sort roots' input copies
+    std::function<int()> after_sorts;    // issues the sort roots' output copies
+    bool halve_light = false;            // the other roots in two launches of alternate roots, one on
+                                         // each side of the sorts
+};
+
+// A batch launch (the caller holds g_mu and has checked the arguments): the
+// roots in admission order in g.d_roots, one launch or a split into
+// segments, results back in the caller's order.
+int run_batch(const gtap_root* roots, int n_roots, gtap_root_result* results, gtap_run_stats* stats,
+              cudaStream_t s, const BatchHooks* hooks) {
+    if (g.h_report) memset(g.h_report, 0, sizeof(GtapErrorReport));
+    int rc = ensure_root_capacity(n_roots);
+    if (rc) return rc;
+    const bool sorts = roots_need_sorts(roots, n_roots);
+    if (!block_mode() && sorts && g.workers_full == 0) return GTAP_ERROR_INVALID_ARGUMENT;
+
+    // admission order: slot i of the device table holds the caller's root order[i]
+    std::vector<int> order;
+    int n_light = sorts ? 0 : n_roots;
+    if (g.cfg.admit_order != GTAP_ADMIT_AS_GIVEN) n_light = admission_order(roots, n_roots, order);
+    const bool split = !block_mode() && g.cfg.admit_order == GTAP_ADMIT_SPLIT && g.cfg.profile_samples == 0 &&
+                       n_light > 0 && n_light < n_roots;
+    const bool halves = split && hooks && hooks->halve_light && n_light >= 2;
+    if (halves) {
+        // two launches of about equal work: alternate roots of the grouped
+        // order, so that each half keeps the grouping and gets half of each kind
+        if (order.empty()) {
+            order.resize(n_roots);
+            for (int i = 0; i < n_roots; ++i) order[i] = i;
+        }
+        std::vector<int> light(order.begin(), order.begin() + n_light);
+        int w = 0;
+        for (int i = 0; i < n_light; i += 2) order[w++] = light[i];
+        for (int i = 1; i < n_light; i += 2) order[w++] = light[i];
+    }
+    const gtap_root* table = roots;
+    std::vector<gtap_root> permuted;
+    if (!order.empty()) {
+        permuted.resize(n_roots);
+        for (int i = 0; i < n_roots; ++i) permuted[i] = roots[order[i]];
+        table = permuted.data();
+    }
+    GT_CUDA(cudaMemcpyAsync(g.d_roots, table, sizeof(gtap_root) * n_roots, cudaMemcpyHostToDevice, s));
+    // the inputs' copies queue behind the root table on the copy engine, so
+    // that a long one does not hold up the first launch
+    if (hooks && hooks->before_launches) {
+        int hc = hooks->before_launches();
+        if (hc) return hc;
+    }
+
+    // segments: one launch, or (split) the kernel without sort leaves over
+    // slots [0, n_light) and the sort-capable kernel over [n_light, n_roots)
+    struct Segment {
+        int first, count;
+        bool light;
+    };
+    std::vector<Segment> segs;
+    if (!split) {
+        segs.push_back({0, n_roots, !sorts});
+    } else if (halves) {
+        const int a = (n_light + 1) / 2;
+        segs = {{0, a, true}, {n_light, n_roots - n_light, false}, {a, n_light - a, true}};
+    } else {
+        segs = {{0, n_light, true}, {n_light, n_roots - n_light, false}};
+    }
+
+    double ms_total = 0, ms_light = 0;
+    int st = 0, launches = 0, light_workers = 0;
+    std::vector<char> ran(n_roots, 0);
+    gtap_run_stats acc{}, shape{};
+    bool have_shape = false;
+    for (const Segment& sg : segs) {
+        const bool needs_sorts = !sg.light || block_mode();
+        if (needs_sorts && hooks && hooks->sort_inputs) GT_CUDA(cudaStreamWaitEvent(s, hooks->sort_inputs, 0));
+        float ms = 0.f;
+        const int stride = block_mode() ? 0 : record_stride_for(table + sg.first, sg.count);
+        st = launch_resident(sg.count, s, &ms, sg.light && !block_mode(), sg.first, stride);
+        ++launches;
+        ms_total += ms;
+        for (int i = sg.first; i < sg.first + sg.count; ++i) ran[i] = 1;
+        if (sg.light && !block_mode()) {
+            ms_light += ms;
+            light_workers = g.last_workers;
+        }
+        if (stats) {
+            gtap_run_stats one{};
+            int cs = collect_stats(&one);
+            if (cs) return cs;
+            for (int k = 0; k < GTAP_STAT_COUNT; ++k) acc.counters[k] += one.counters[k];
+            if (!have_shape || !sg.light) shape = one;   // the sort-capable launch's shape, if one ran
+            have_shape = true;
+        }
+        if (st != 0) break;
+        if (!sg.light && hooks && hooks->after_sorts) {
+            st = hooks->after_sorts();
+            if (st != 0) break;
+        }
+    }
+
+    if (results) {
+        gtap_root_result* dst = results;
+        std::vector<gtap_root_result> staged;
+        if (!order.empty()) {
+            staged.resize(n_roots);
+            dst = staged.data();
+        }
+        GT_CUDA(cudaMemcpyAsync(dst, g.d_results, sizeof(gtap_root_result) * n_roots, cudaMemcpyDeviceToHost, s));
+        GT_CUDA(cudaStreamSynchronize(s));
+        for (int i = 0; i < n_roots; ++i) {
+            if (!ran[i]) {   // a segment after a failed launch: never admitted
+                dst[i] = gtap_root_result{};
+                dst[i].status = GTAP_ROOT_PENDING;
+            }
+            const int caller = order.empty() ? i : order[i];
+            dst[i].index = caller;
+            if (!order.empty()) results[caller] = dst[i];
+        }
+    }
+    if (stats) {
+        *stats = shape;
+        for (int k = 0; k < GTAP_STAT_COUNT; ++k) stats->counters[k] = acc.counters[k];
+        stats->kernel_ms = ms_total;
+        stats->status = st;
+        stats->launches = launches;
+        stats->light_workers = light_workers;
+        stats->light_kernel_ms = ms_light;
+    }
+    return st;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -464,6 +661,7 @@ int gtap_default_config(gtap_config* cfg) {
     cfg->result_handles = 1000;
     cfg->publish_lazy = 0;
     cfg->max_inflight_roots = 0;
+    cfg->admit_order = GTAP_ADMIT_SPLIT;
     return 0;
 }
 
@@ -716,25 +914,7 @@ int gtap_launch(const gtap_root* roots, int32_t n_roots, gtap_root_result* resul
     if (!g.initialized) return GTAP_ERROR_NOT_INITIALIZED;
     if (g.serving) return GTAP_ERROR_BUSY;
     if (!roots || n_roots < 1) return GTAP_ERROR_INVALID_ARGUMENT;
-    if (g.h_report) memset(g.h_report, 0, sizeof(GtapErrorReport));
-    int rc = ensure_root_capacity(n_roots);
-    if (rc) return rc;
-    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    if (!block_mode() && roots_need_sorts(roots, n_roots) && g.workers_full == 0) return GTAP_ERROR_INVALID_ARGUMENT;
-    GT_CUDA(cudaMemcpyAsync(g.d_roots, roots, sizeof(gtap_root) * n_roots, cudaMemcpyHostToDevice, s));
-    float ms = 0.f;
-    int st = launch_resident(n_roots, s, &ms, !roots_need_sorts(roots, n_roots));
-    if (results) {
-        GT_CUDA(cudaMemcpyAsync(results, g.d_results, sizeof(gtap_root_result) * n_roots, cudaMemcpyDeviceToHost, s));
-        GT_CUDA(cudaStreamSynchronize(s));
-    }
-    if (stats) {
-        int cs = collect_stats(stats);
-        if (cs) return cs;
-        stats->kernel_ms = ms;
-        stats->status = st;
-    }
-    return st;
+    return run_batch(roots, n_roots, results, stats, reinterpret_cast<cudaStream_t>(stream), nullptr);
 }
 
 int gtap_launch_per_root(const gtap_root* roots, int32_t n_roots, gtap_root_result* results,
@@ -747,14 +927,20 @@ int gtap_launch_per_root(const gtap_root* roots, int32_t n_roots, gtap_root_resu
     if (rc) return rc;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     gtap_run_stats total{};
-    double ms_total = 0;
-    int st = 0;
+    double ms_total = 0, ms_light = 0;
+    int st = 0, launches = 0, light_workers = 0;
     for (int i = 0; i < n_roots && st == 0; ++i) {
         GT_CUDA(cudaMemcpyAsync(g.d_roots, roots + i, sizeof(gtap_root), cudaMemcpyHostToDevice, s));
         float ms = 0.f;
-        if (!block_mode() && roots_need_sorts(roots + i, 1) && g.workers_full == 0) return GTAP_ERROR_INVALID_ARGUMENT;
-        st = launch_resident(1, s, &ms, !roots_need_sorts(roots + i, 1));
+        const bool light = !roots_need_sorts(roots + i, 1);
+        if (!block_mode() && !light && g.workers_full == 0) return GTAP_ERROR_INVALID_ARGUMENT;
+        st = launch_resident(1, s, &ms, light);
         ms_total += ms;
+        ++launches;
+        if (light && !block_mode()) {
+            ms_light += ms;
+            light_workers = g.last_workers;
+        }
         if (results) {
             GT_CUDA(cudaMemcpyAsync(results + i, g.d_results, sizeof(gtap_root_result), cudaMemcpyDeviceToHost, s));
         }
@@ -775,6 +961,9 @@ int gtap_launch_per_root(const gtap_root* roots, int32_t n_roots, gtap_root_resu
         stats->block = g.cfg.block;
         stats->workers = g.last_workers;
         stats->status = st;
+        stats->launches = launches;
+        stats->light_workers = light_workers;
+        stats->light_kernel_ms = ms_light;
     }
     return st;
 }
@@ -785,30 +974,94 @@ int gtap_launch_per_root(const gtap_root* roots, int32_t n_roots, gtap_root_resu
 // host-buffer entry point
 // ---------------------------------------------------------------------------
 namespace {
+// One root array of a host-buffer batch and its place in the device slab.
 struct HostCopy {
-    void* host;
+    void* host;   // null: device scratch only
     size_t off;
     size_t bytes;
-    bool in;    // copy host -> device before the launch
-    bool out;   // copy device -> host after the launch
+    bool in;      // copied host -> device before the root runs
+    bool out;     // copied device -> host after it ran
+    bool sort;    // belongs to a sort root
 };
+
+// Slab layout: arrays of one class (sort or not, in / out / in-out /
+// scratch) in plan order, and an array that continues the previous one of
+// its class in host memory continues it in the slab too, so that a batch whose
+// roots slice one host buffer moves it in one copy each way.  Other arrays
+// start on 256-byte boundaries.  Returns the slab size.
+size_t layout_slab(std::vector<HostCopy>& copies) {
+    size_t total = 0;
+    for (int cls = 0; cls < 8; ++cls) {
+        const HostCopy* prev = nullptr;
+        for (auto& c : copies) {
+            const int k = (c.sort ? 4 : 0) + (c.in ? 2 : 0) + (c.out ? 1 : 0);
+            if (k != cls) continue;
+            const bool follows = prev && c.host && prev->host &&
+                                 static_cast<const char*>(prev->host) + prev->bytes == c.host &&
+                                 prev->off + prev->bytes == total;
+            c.off = follows ? total : (total + 255) & ~(size_t)255;
+            total = c.off + c.bytes;
+            prev = &c;
+        }
+    }
+    return total;
+}
+
+// Issue the copies of one direction and class, one per run of arrays that
+// are contiguous on both sides.
+int issue_copies(const std::vector<HostCopy>& copies, char* slab, bool to_device, bool sort, cudaStream_t s,
+                 int64_t& bytes) {
+    size_t run_off = 0, run_bytes = 0;
+    const char* run_host = nullptr;
+    auto flush = [&]() -> int {
+        if (!run_bytes) return 0;
+        cudaError_t e = to_device ? cudaMemcpyAsync(slab + run_off, run_host, run_bytes, cudaMemcpyHostToDevice, s)
+                                  : cudaMemcpyAsync(const_cast<char*>(run_host), slab + run_off, run_bytes,
+                                                    cudaMemcpyDeviceToHost, s);
+        if (e != cudaSuccess) return -(int)e;
+        bytes += (int64_t)run_bytes;
+        run_bytes = 0;
+        return 0;
+    };
+    for (int cls = 0; cls < 8; ++cls) {   // the layout's order, so that runs meet
+        for (const auto& c : copies) {
+            const int k = (c.sort ? 4 : 0) + (c.in ? 2 : 0) + (c.out ? 1 : 0);
+            if (k != cls || c.sort != sort || !(to_device ? c.in : c.out)) continue;
+            const char* h = static_cast<const char*>(c.host);
+            if (run_bytes && run_host + run_bytes == h && run_off + run_bytes == c.off) {
+                run_bytes += c.bytes;
+                continue;
+            }
+            int rc = flush();
+            if (rc) return rc;
+            run_host = h;
+            run_off = c.off;
+            run_bytes = c.bytes;
+        }
+        int rc = flush();
+        if (rc) return rc;
+    }
+    return 0;
+}
 }  // namespace
 
 extern "C" int gtap_run_host(const gtap_root* roots, int32_t n_roots, gtap_root_result* results,
                              gtap_run_stats* stats, int64_t* h2d_bytes, int64_t* d2h_bytes) {
     if (!roots || n_roots < 1) return GTAP_ERROR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(g_mu);
     if (!g.initialized) return GTAP_ERROR_NOT_INITIALIZED;
+    if (g.serving) return GTAP_ERROR_BUSY;
     std::vector<gtap_root> dev_roots(roots, roots + n_roots);
     std::vector<HostCopy> copies;
-    size_t total = 0;
+    bool sort_root = false;
     auto plan = [&](void* host, size_t bytes, bool in, bool out) -> int {
-        copies.push_back(HostCopy{host, total, bytes, in && host != nullptr, out && host != nullptr});
-        total += (bytes + 255) & ~(size_t)255;
+        copies.push_back(HostCopy{host, 0, bytes, in && host != nullptr, out && host != nullptr, sort_root});
         return (int)copies.size() - 1;
     };
     std::vector<std::vector<int>> idx(n_roots);
     for (int i = 0; i < n_roots; ++i) {
         const gtap_root& r = roots[i];
+        sort_root = is_sort_kind(r.kind);
         switch (r.kind) {
             case GTAP_KIND_CILKSORT:
             case GTAP_KIND_MERGESORT: {
@@ -834,6 +1087,7 @@ extern "C" int gtap_run_host(const gtap_root* roots, int32_t n_roots, gtap_root_
                 break;
         }
     }
+    const size_t total = layout_slab(copies);
     if (total > g_slab_bytes) {
         if (g_slab) cudaFree(g_slab);
         g_slab = nullptr;
@@ -842,33 +1096,58 @@ extern "C" int gtap_run_host(const gtap_root* roots, int32_t n_roots, gtap_root_
         if (e != cudaSuccess) return -(int)e;
         g_slab_bytes = total;
     }
-    int64_t hin = 0, hout = 0;
-    cudaStream_t s = nullptr;
-    for (auto& c : copies) {
-        if (c.in) {
-            GT_CUDA(cudaMemcpyAsync(g_slab + c.off, c.host, c.bytes, cudaMemcpyHostToDevice, s));
-            hin += (int64_t)c.bytes;
-        }
-    }
     for (int i = 0; i < n_roots; ++i) {
         gtap_root& r = dev_roots[i];
         const std::vector<int>& k = idx[i];
         void** ps[4] = {&r.p0, &r.p1, &r.p2, &r.p3};
         for (size_t j = 0; j < k.size(); ++j) *ps[j] = g_slab + copies[k[j]].off;
     }
-    int st = gtap_launch(dev_roots.data(), n_roots, results, stats, nullptr);
-    for (auto& c : copies) {
-        if (c.out) {
-            GT_CUDA(cudaMemcpyAsync(c.host, g_slab + c.off, c.bytes, cudaMemcpyDeviceToHost, s));
-            hout += (int64_t)c.bytes;
-        }
+
+    // the other roots' inputs on the launch stream; the sorts' inputs and
+    // outputs on a copy stream that runs beside the launches (the copies
+    // overlap them when the host buffers are pinned)
+    int64_t hin = 0, hout = 0;
+    cudaStream_t s = nullptr, cs = nullptr;
+    cudaEvent_t in_done = nullptr, sorted = nullptr;
+    GT_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    GT_CUDA(cudaEventCreateWithFlags(&in_done, cudaEventDisableTiming));
+    GT_CUDA(cudaEventCreateWithFlags(&sorted, cudaEventDisableTiming));
+    int st = 0;
+    bool inputs_in = false;   // no output is copied back unless its inputs went in
+    {
+        BatchHooks hooks;
+        hooks.before_launches = [&]() -> int {
+            int rc = issue_copies(copies, g_slab, true, false, s, hin);
+            if (rc == 0) rc = issue_copies(copies, g_slab, true, true, cs, hin);
+            if (rc == 0 && cudaEventRecord(in_done, cs) != cudaSuccess) rc = GTAP_ERROR_INVALID_ARGUMENT;
+            inputs_in = rc == 0;
+            return rc;
+        };
+        hooks.sort_inputs = in_done;
+        hooks.halve_light = true;
+        hooks.after_sorts = [&]() -> int {
+            if (cudaEventRecord(sorted, s) != cudaSuccess || cudaStreamWaitEvent(cs, sorted, 0) != cudaSuccess)
+                return GTAP_ERROR_INVALID_ARGUMENT;
+            return issue_copies(copies, g_slab, false, true, cs, hout);
+        };
+        st = run_batch(dev_roots.data(), n_roots, results, stats, s, &hooks);
+        // sorts that never ran (a failed earlier launch) leave their outputs unwritten
+    }
+    if (inputs_in) {
+        int oc = issue_copies(copies, g_slab, false, false, s, hout);
+        if (st == 0) st = oc;
     }
     cudaError_t e = cudaStreamSynchronize(s);
+    cudaError_t e2 = cudaStreamSynchronize(cs);
+    cudaStreamDestroy(cs);
+    cudaEventDestroy(in_done);
+    cudaEventDestroy(sorted);
     hin += (int64_t)sizeof(gtap_root) * n_roots;
     if (results) hout += (int64_t)sizeof(gtap_root_result) * n_roots;
     if (h2d_bytes) *h2d_bytes = hin;
     if (d2h_bytes) *d2h_bytes = hout;
     if (e != cudaSuccess && st == 0) return -(int)e;
+    if (e2 != cudaSuccess && st == 0) return -(int)e2;
     return st;
 }
 
@@ -1352,6 +1631,14 @@ extern "C" int gtap_selftest_queues(int32_t rounds, int32_t per_round_max, int32
 // ---------------------------------------------------------------------------
 namespace gtap {
 int noalloc_set_ring_position(uint32_t position);   // gtap_noalloc.cu
+}
+
+extern "C" int gtap_debug_admission_order(const gtap_root* roots, int32_t n, int32_t* order, int32_t* n_light) {
+    if (!roots || n < 0 || !order || !n_light) return GTAP_ERROR_INVALID_ARGUMENT;
+    std::vector<int> o;
+    *n_light = admission_order(roots, n, o);
+    for (int i = 0; i < n; ++i) order[i] = o.empty() ? i : o[i];
+    return 0;
 }
 
 extern "C" int gtap_debug_set_ring_position(int32_t target, uint32_t position) {

@@ -48,8 +48,11 @@ int gtap_get_config(gtap_config* out);
 /* launches (NEW; the reference launches exec_kernel<<<GRID,BLOCK>>> with   */
 /* one root pushed by __gtap_push_initial_task, gtap_runtime_thread.cuh:818) */
 /* ------------------------------------------------------------------------ */
-/* Run n_roots roots (device-resident inputs) in ONE persistent launch on the
- * given CUDA stream (NULL = default) and wait for it.  results may be NULL. */
+/* Run n_roots roots (device-resident inputs) in one persistent launch on the
+ * given CUDA stream (NULL = default) and wait for it; under GTAP_ADMIT_SPLIT
+ * (the default) a thread-mode batch that mixes sorts with other kinds runs as
+ * two launches back to back (gtap_types.h).  results may be NULL; they are
+ * returned in the order of roots, results[i].index == i. */
 int gtap_launch(const gtap_root* roots, int32_t n_roots, gtap_root_result* results, gtap_run_stats* stats,
                 void* stream);
 /* The plain per-root baseline: gtap_reset() + one launch per root, as the
@@ -57,9 +60,14 @@ int gtap_launch(const gtap_root* roots, int32_t n_roots, gtap_root_result* resul
 int gtap_launch_per_root(const gtap_root* roots, int32_t n_roots, gtap_root_result* results,
                          gtap_run_stats* stats, void* stream);
 /* Host-buffer entry point: root pointers refer to HOST memory.  Arrays are
- * copied to the device, the roots run in one launch, and outputs (sorted
- * arrays, BFS depths) are copied back into the same host buffers.
- * h2d_bytes / d2h_bytes (optional) report the bytes moved. */
+ * copied to the device, the roots run, and outputs (sorted arrays, BFS
+ * depths) are copied back into the same host buffers; arrays that continue
+ * one another in host memory move in one copy.  Under GTAP_ADMIT_SPLIT a
+ * batch of sorts and other kinds runs in three launches: half of the other
+ * roots while the sorts' keys are copied in, the sorts, then the other half
+ * while the sorted keys are copied out (the copies overlap the launches when
+ * the host buffers are pinned).  h2d_bytes / d2h_bytes (optional) report the
+ * bytes moved. */
 int gtap_run_host(const gtap_root* roots, int32_t n_roots, gtap_root_result* results, gtap_run_stats* stats,
                   int64_t* h2d_bytes, int64_t* d2h_bytes);
 
@@ -134,6 +142,12 @@ int gtap_get_arena_counters(int64_t* out, int32_t n);
  * gtap_initialize() (between launches); target 1: the scratch array of
  * gtap_launch_noalloc() on the current device (after its first call). */
 int gtap_debug_set_ring_position(int32_t target, uint32_t position);
+
+/* Test aid, host only (no device call): the admission order gtap_launch
+ * gives a batch under GTAP_ADMIT_BY_KIND / GTAP_ADMIT_SPLIT.  order[i] = the
+ * caller's index of the root admitted i-th (n entries); *n_light = the roots
+ * ahead of the first sort (the first launch of a split batch). */
+int gtap_debug_admission_order(const gtap_root* roots, int32_t n, int32_t* order, int32_t* n_light);
 
 /* No counterpart in the reference.  For callers that cannot allocate device
  * memory (a serving loop that must avoid an allocation's implicit device-wide

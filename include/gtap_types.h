@@ -87,7 +87,21 @@ typedef struct gtap_config {
     int32_t publish_lazy;    /* 0: publish every task beyond the next batch each round (reference push_batch);
                                 1: keep up to 128 ready tasks per queue private until some worker is idle */
     int32_t max_inflight_roots; /* roots admitted but not finished, at most; 0 = no limit */
+    int32_t admit_order;     /* GTAP_ADMIT_*: the order in which a batch launch admits its roots */
 } gtap_config;
+
+/* Admission order of a batch (gtap_launch, gtap_run_host).  Results come back
+   in the caller's order whatever the admission order.
+   AS_GIVEN:   the roots' order, one persistent launch.
+   BY_KIND:    a stable grouping by kind (fib, n-queens, BFS, tree sums, then
+               the sorts), one persistent launch: the warps of an SM then run
+               one task body at a time instead of all of them at once.
+   SPLIT:      BY_KIND, and a thread-mode batch that mixes sorts with other
+               kinds runs as two launches back to back on the stream: the
+               kernel without sort leaves (more warps per SM, fewer registers)
+               over the other kinds, then the sort-capable kernel over the
+               sorts.  Block mode admits BY_KIND. */
+enum { GTAP_ADMIT_AS_GIVEN = 0, GTAP_ADMIT_BY_KIND = 1, GTAP_ADMIT_SPLIT = 2 };
 
 /* ------------------------------------------------------------------------ */
 /* built-in task kinds and root descriptors (NEW)                           */
@@ -143,10 +157,13 @@ enum {
 };
 
 typedef struct gtap_run_stats {
-    uint64_t counters[GTAP_STAT_COUNT];
-    double kernel_ms;        /* CUDA-event time of the persistent launch */
-    int32_t grid, block, workers;
+    uint64_t counters[GTAP_STAT_COUNT];   /* summed over the launches */
+    double kernel_ms;        /* CUDA-event time of the persistent launch(es), summed */
+    int32_t grid, block, workers;   /* of the sort-capable launch when one ran, else of the last launch */
     int32_t status;
+    int32_t launches;        /* persistent worker launches (2 for a split batch, GTAP_ADMIT_SPLIT) */
+    int32_t light_workers;   /* workers of the launch without sort leaves, 0 if none ran */
+    double light_kernel_ms;  /* part of kernel_ms spent in that launch */
 } gtap_run_stats;
 
 #ifdef __cplusplus

@@ -77,3 +77,14 @@ def test_reference_arm_runs_without_the_product_library():
     import gtap_b200 as gt
     from gtap_b200.workloads import Mix
     assert line["config"] == bench.workload_config(Mix(gt, 96))
+
+
+def test_worker_kernels_of_a_split_and_an_unsplit_step():
+    split = bench.worker_kernels(100e6, 200e6, 50.0, 25.0, 6000.0)
+    assert [k["kernel"] for k in split] == [bench.LIGHT_KERNEL, bench.FULL_KERNEL]
+    assert [k["algorithmic_bytes"] for k in split] == [100e6, 200e6]
+    assert abs(split[0]["achieved_gbs"] - 2.0) < 1e-9 and abs(split[1]["frac"] - 8.0 / 6000.0) < 1e-12
+    one = bench.worker_kernels(100e6, 200e6, 0.0, 75.0, 6000.0)
+    assert len(one) == 1 and one[0]["kernel"] == bench.FULL_KERNEL and one[0]["algorithmic_bytes"] == 300e6
+    only_light = bench.worker_kernels(100e6, 0, 40.0, 0.0, 6000.0)
+    assert [k["kernel"] for k in only_light] == [bench.LIGHT_KERNEL]

@@ -43,8 +43,11 @@ def test_struct_layouts_match_header():
     # sizes the C side uses (checked through offsets of the last fields)
     assert ctypes.sizeof(gt.Root) == 56
     assert ctypes.sizeof(gt.RootResult) == 40
-    assert ctypes.sizeof(gt.Config) == 80
+    assert ctypes.sizeof(gt.Config) == 88
     assert gt.Config.total_ids.offset == 40
+    assert gt.Config.admit_order.offset == 80
+    assert ctypes.sizeof(gt.RunStats) == 168
+    assert gt.RunStats.light_kernel_ms.offset == 160
 
 
 def test_default_config():
