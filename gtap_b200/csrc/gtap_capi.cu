@@ -45,6 +45,7 @@ struct Runtime {
     int workers = 0;            // arena capacity: max over the kernel variants
     int workers_full = 0;       // thread_worker_kernel<BuiltinProgram>
     int workers_light = 0;      // thread_worker_kernel_lb<BuiltinProgramLight>
+    bool fibnq_ok = false;      // thread_worker_kernel_lb<BuiltinProgramFibNq> fits as many workers
     int workers_block = 0;      // block_worker_kernel<BlockProgram>: one worker per block (block mode only)
     int last_workers = 0;       // workers of the last launch
     bool last_block = false;    // the last launch ran the block kernel
@@ -139,6 +140,10 @@ const void* kernel_light(int num_queues) {
     return num_queues == 1 ? reinterpret_cast<const void*>(&thread_worker_kernel_lb<BuiltinProgramLight, 1>)
                            : reinterpret_cast<const void*>(&thread_worker_kernel_lb<BuiltinProgramLight, kMaxQueues>);
 }
+const void* kernel_fibnq(int num_queues) {
+    return num_queues == 1 ? reinterpret_cast<const void*>(&thread_worker_kernel_lb<BuiltinProgramFibNq, 1>)
+                           : reinterpret_cast<const void*>(&thread_worker_kernel_lb<BuiltinProgramFibNq, kMaxQueues>);
+}
 
 // Roots are admitted while at least this many task ids are free (never used
 // or recycled).  Ids parked in private ranges and per-warp caches are not
@@ -170,6 +175,12 @@ static_assert(sizeof(prog::FibFrame) <= 16 && sizeof(prog::NqFrame) <= 16 && siz
               "16-byte frames");
 int frame_bytes_of(int kind) {
     return (kind == GTAP_KIND_FIB || kind == GTAP_KIND_NQ || kind == GTAP_KIND_BFS) ? 16 : BuiltinProgram::kFrameBytes;
+}
+
+bool only_fib_nq(const gtap_root* roots, int n) {
+    for (int i = 0; i < n; ++i)
+        if (roots[i].kind != GTAP_KIND_FIB && roots[i].kind != GTAP_KIND_NQ) return false;
+    return true;
 }
 
 // Record stride of a launch over roots[0, n): the configured one, or less
@@ -213,14 +224,20 @@ constexpr size_t kBlockSmemBytes = (size_t)BlockProgram::kSmemInts * sizeof(int)
 
 bool block_mode() { return g.cfg.mode == GTAP_MODE_BLOCK; }
 
-// launch the worker kernel variant; A.num_workers must match it
-cudaError_t launch_worker(const Arena& A, bool light, cudaStream_t s) {
+// launch the worker kernel variant; A.num_workers must match it.  fibnq:
+// the light kernel without the BFS and tree-sum bodies (same occupancy).
+cudaError_t launch_worker(const Arena& A, bool light, cudaStream_t s, bool fibnq = false) {
     if (block_mode()) {
         block_worker_kernel<BlockProgram><<<A.num_workers, g.cfg.block, kBlockSmemBytes, s>>>(A);
         return cudaGetLastError();
     }
     const int blocks = A.num_workers / g.warps_per_block;
     const bool one = g.cfg.num_queues == 1;
+    if (light && fibnq && g.fibnq_ok) {
+        if (one) thread_worker_kernel_lb<BuiltinProgramFibNq, 1><<<blocks, g.cfg.block, g.smem_bytes, s>>>(A);
+        else thread_worker_kernel_lb<BuiltinProgramFibNq, kMaxQueues><<<blocks, g.cfg.block, g.smem_bytes, s>>>(A);
+        return cudaGetLastError();
+    }
     if (light && one) thread_worker_kernel_lb<BuiltinProgramLight, 1><<<blocks, g.cfg.block, g.smem_bytes, s>>>(A);
     else if (light) thread_worker_kernel_lb<BuiltinProgramLight, kMaxQueues><<<blocks, g.cfg.block, g.smem_bytes, s>>>(A);
     else if (one) thread_worker_kernel<BuiltinProgram, 1><<<blocks, g.cfg.block, g.smem_full, s>>>(A);
@@ -435,7 +452,8 @@ int collect_stats(gtap_run_stats* stats) {
 
 // One persistent launch over the roots already in g.d_roots[first_root, first_root + n_roots).
 // rec_stride > 0: the record stride of this launch (at most the configured one).
-int launch_resident(int n_roots, cudaStream_t s, float* ms_out, bool light, int first_root = 0, int rec_stride = 0) {
+int launch_resident(int n_roots, cudaStream_t s, float* ms_out, bool light, int first_root = 0, int rec_stride = 0,
+                    bool fibnq = false) {
     if (g.cfg.profile_samples > 0) {
         size_t n = (size_t)g.workers * g.cfg.profile_samples;
         GT_CUDA(cudaMemsetAsync(g.prof_having, 0, n * sizeof(long long), s));
@@ -461,7 +479,7 @@ int launch_resident(int n_roots, cudaStream_t s, float* ms_out, bool light, int 
     GT_CUDA(cudaEventCreate(&e0));
     GT_CUDA(cudaEventCreate(&e1));
     GT_CUDA(cudaEventRecord(e0, s));
-    cudaError_t le = launch_worker(A, light, s);
+    cudaError_t le = launch_worker(A, light, s, fibnq);
     GT_CUDA(cudaEventRecord(e1, s));
     cudaError_t se = cudaEventSynchronize(e1);
     float ms = 0.f;
@@ -573,7 +591,8 @@ int run_batch(const gtap_root* roots, int n_roots, gtap_root_result* results, gt
         if (needs_sorts && hooks && hooks->sort_inputs) GT_CUDA(cudaStreamWaitEvent(s, hooks->sort_inputs, 0));
         float ms = 0.f;
         const int stride = block_mode() ? 0 : record_stride_for(table + sg.first, sg.count);
-        st = launch_resident(sg.count, s, &ms, sg.light && !block_mode(), sg.first, stride);
+        st = launch_resident(sg.count, s, &ms, sg.light && !block_mode(), sg.first, stride,
+                             only_fib_nq(table + sg.first, sg.count));
         ++launches;
         ms_total += ms;
         for (int i = sg.first; i < sg.first + sg.count; ++i) ran[i] = 1;
@@ -697,6 +716,12 @@ static int initialize_impl(const gtap_config* cfg_in, int external_workers) {
         GT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_full, kernel_full(c.num_queues), c.block, smem_full));
     GT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_light, kernel_light(c.num_queues), c.block, smem));
     if (per_sm_light < 1) return GTAP_ERROR_INVALID_ARGUMENT;
+    {
+        int per_sm_fibnq = 0;
+        GT_CUDA(cudaFuncSetAttribute(kernel_fibnq(c.num_queues), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        GT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_fibnq, kernel_fibnq(c.num_queues), c.block, smem));
+        g.fibnq_ok = per_sm_fibnq >= per_sm_light;
+    }
     // one resident wave per variant; grid = 0 fills the GPU, otherwise cap it
     auto pick = [&](int per_sm) {
         int cap = per_sm * g.sm_count;

@@ -776,8 +776,10 @@ __device__ __forceinline__ void treesum_task(const Arena& A, WarpShared& S, void
 // Program: dispatch by kind (a switch, not an indirect call)
 // ---------------------------------------------------------------------------
 // kSorts = false leaves the register-heavy sorting kinds out of the kernel,
-// which lets fib / n-queens / BFS / tree launches run at higher occupancy.
-template <bool kSorts>
+// which lets fib / n-queens / BFS / tree launches run at higher occupancy;
+// kGraphs = false also leaves out BFS and tree sums, so that a launch of fib
+// and n-queens roots runs a kernel with two task bodies.
+template <bool kSorts, bool kGraphs = true>
 struct BuiltinProgramT {
     static constexpr int kFrameBytes = prog::kFrameBytes;
     static constexpr bool kFrameWords = true;    // exec gets the first 32 frame bytes
@@ -968,8 +970,14 @@ struct BuiltinProgramT {
                 if (kSorts) prog::mergesort_task(A, S, frame, w0, w1);
                 else { GTAP_ERROR(A, ERR_INVALID_KIND, tid, -1, kind, 0); rt_finish(S); }
                 break;
-            case prog::K_BFS: prog::bfs_task(A, S, frame, w0); break;
-            case prog::K_TREESUM: prog::treesum_task(A, S, frame, w0, w1); break;
+            case prog::K_BFS:
+                if constexpr (kGraphs) prog::bfs_task(A, S, frame, w0);
+                else { GTAP_ERROR(A, ERR_INVALID_KIND, tid, -1, kind, 0); rt_finish(S); }
+                break;
+            case prog::K_TREESUM:
+                if constexpr (kGraphs) prog::treesum_task(A, S, frame, w0, w1);
+                else { GTAP_ERROR(A, ERR_INVALID_KIND, tid, -1, kind, 0); rt_finish(S); }
+                break;
             default:
                 GTAP_ERROR(A, ERR_INVALID_KIND, tid, -1, kind, 0);
                 rt_finish(S);
@@ -980,5 +988,6 @@ struct BuiltinProgramT {
 
 using BuiltinProgram = BuiltinProgramT<true>;
 using BuiltinProgramLight = BuiltinProgramT<false>;
+using BuiltinProgramFibNq = BuiltinProgramT<false, false>;
 
 }  // namespace gtap
