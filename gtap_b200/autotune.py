@@ -16,6 +16,10 @@ Search: coordinate descent from the library defaults over
   num_queues     EPAQ queues
   spawn_capacity children staged per worker and round (shared memory per warp,
                  so it also sets how many workers fit an SM)
+  max_inflight_roots  roots admitted and not finished, at most (0: no limit);
+                 an asynchronous BFS relaxes vertices more than once the more
+                 roots share the GPU, so served batches of BFS roots do less
+                 work with fewer of them in flight
 Each trial re-initialises the runtime with the candidate configuration, runs
 one warm-up launch and `reps` timed launches (CUDA events around the
 persistent kernel) and keeps the median.  Every trial's results must equal the
@@ -27,9 +31,10 @@ configuration that breaks a result cannot win.
 
 The serve workload is the served roots (BFS on R-MAT 16-20, tree sums of
 2^18-2^20 nodes, 200 of them) in one batch launch of the kernel serve mode
-runs, the session's capacity when every root arrives at once; BFS depth arrays
-are reset before every launch, and a BFS root's task count (timing-dependent)
-is left out of the result check.
+runs, the session's capacity when every root arrives at once, admitted in
+arrival order as a session admits them; BFS depth arrays are reset before
+every launch, and a BFS root's task count (timing-dependent) is left out of
+the result check.
 """
 import argparse
 import json
@@ -47,9 +52,10 @@ SPACE = {
     "victim_policy": [0, 1, 2],
     "num_queues": [1, 2, 4],
     "spawn_capacity": [128, 256, 512, 1024],
+    "max_inflight_roots": [0, 8, 16, 32, 64, 128],
 }
-ORDER = ["warps_per_sm", "block", "steal_batch", "deque_capacity", "probe_width", "victim_policy", "num_queues",
-         "spawn_capacity"]
+ORDER = ["max_inflight_roots", "warps_per_sm", "block", "steal_batch", "deque_capacity", "probe_width",
+         "victim_policy", "num_queues", "spawn_capacity"]
 
 
 def to_overrides(point, sm_count):
@@ -116,6 +122,7 @@ def run(workload="mix", reps=3, sweeps=2, n_roots=None, out=None, quiet=False, s
     sm_count = torch.cuda.get_device_properties(0).multi_processor_count
     keep = []
     before = None   # runs before every launch (resets what a launch consumes)
+    fixed = {}      # overrides every trial carries
     if workload == "mix":
         mix = wl.Mix(gt, n_roots or wl.N_ROOTS)
         src, arr, tmp = mix.device_slabs()
@@ -129,6 +136,7 @@ def run(workload="mix", reps=3, sweeps=2, n_roots=None, out=None, quiet=False, s
         sw = ServeWorkload(gt)
         roots, depths = sw.roots(sw.draw(n_roots or 200))
         keep += [sw, depths]
+        fixed["admit_order"] = gt.ADMIT_AS_GIVEN
 
         def before():
             for d in depths:
@@ -143,6 +151,7 @@ def run(workload="mix", reps=3, sweeps=2, n_roots=None, out=None, quiet=False, s
 
     def measure(point):
         over = to_overrides(point, sm_count)
+        over.update(fixed)
         try:
             gt.gtap_initialize(gt.default_config(**over))
         except gt.GtapError:
@@ -176,12 +185,14 @@ def run(workload="mix", reps=3, sweeps=2, n_roots=None, out=None, quiet=False, s
     start = {"warps_per_sm": 8, "block": defaults.block, "deque_capacity": defaults.deque_capacity,
              "steal_batch": defaults.steal_batch, "probe_width": defaults.probe_width,
              "victim_policy": defaults.victim_policy, "num_queues": defaults.num_queues,
-             "spawn_capacity": defaults.spawn_capacity}
+             "spawn_capacity": defaults.spawn_capacity, "max_inflight_roots": defaults.max_inflight_roots}
     start.update(start_point or {})
     t0 = time.time()
     best, best_t, trials = coordinate_descent(measure, start, sweeps=sweeps, log=log)
+    best_over = to_overrides(best, sm_count)
+    best_over.update(fixed)
     result = {"workload": workload, "roots": len(roots), "device": torch.cuda.get_device_name(0),
-              "sm_count": sm_count, "best_point": best, "best_overrides": to_overrides(best, sm_count),
+              "sm_count": sm_count, "best_point": best, "best_overrides": best_over,
               "best_kernel_ms": best_t * 1e3, "reps": reps, "trials": len(trials),
               "search_s": time.time() - t0,
               "table": sorted(({"point": t["point"], "kernel_ms": None if t["s"] is None else t["s"] * 1e3}
