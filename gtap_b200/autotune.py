@@ -16,6 +16,9 @@ Search: coordinate descent from the library defaults over
   num_queues     EPAQ queues
   spawn_capacity children staged per worker and round (shared memory per warp,
                  so it also sets how many workers fit an SM)
+  publish_lazy   0: publish every ready task beyond the next batch each round;
+                 1: keep up to a batch in reserve privately until some worker is
+                 idle (fuller rounds once the GPU is busy, a slower ramp-up)
   max_inflight_roots  roots admitted and not finished, at most (0: no limit);
                  an asynchronous BFS relaxes vertices more than once the more
                  roots share the GPU, so served batches of BFS roots do less
@@ -53,8 +56,9 @@ SPACE = {
     "num_queues": [1, 2, 4],
     "spawn_capacity": [128, 256, 512, 1024],
     "max_inflight_roots": [0, 8, 16, 32, 64, 128],
+    "publish_lazy": [0, 1],
 }
-ORDER = ["max_inflight_roots", "warps_per_sm", "block", "steal_batch", "deque_capacity", "probe_width",
+ORDER = ["publish_lazy", "max_inflight_roots", "warps_per_sm", "block", "steal_batch", "deque_capacity", "probe_width",
          "victim_policy", "num_queues", "spawn_capacity"]
 
 
@@ -185,7 +189,8 @@ def run(workload="mix", reps=3, sweeps=2, n_roots=None, out=None, quiet=False, s
     start = {"warps_per_sm": 8, "block": defaults.block, "deque_capacity": defaults.deque_capacity,
              "steal_batch": defaults.steal_batch, "probe_width": defaults.probe_width,
              "victim_policy": defaults.victim_policy, "num_queues": defaults.num_queues,
-             "spawn_capacity": defaults.spawn_capacity, "max_inflight_roots": defaults.max_inflight_roots}
+             "spawn_capacity": defaults.spawn_capacity, "max_inflight_roots": defaults.max_inflight_roots,
+             "publish_lazy": defaults.publish_lazy}
     start.update(start_point or {})
     t0 = time.time()
     best, best_t, trials = coordinate_descent(measure, start, sweeps=sweeps, log=log)
