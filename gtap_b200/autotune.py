@@ -16,6 +16,8 @@ Search: coordinate descent from the library defaults over
   num_queues     EPAQ queues
   spawn_capacity children staged per worker and round (shared memory per warp,
                  so it also sets how many workers fit an SM)
+  leaf_batch     sort and merge leaves a warp stages in shared memory at once
+                 (one load round trip per batch, 1 KB of shared memory each)
   publish_lazy   0: publish every ready task beyond the next batch each round;
                  1: keep up to a batch in reserve privately until some worker is
                  idle (fuller rounds once the GPU is busy, a slower ramp-up)
@@ -57,8 +59,9 @@ SPACE = {
     "spawn_capacity": [128, 256, 512, 1024],
     "max_inflight_roots": [0, 8, 16, 32, 64, 128],
     "publish_lazy": [0, 1],
+    "leaf_batch": [1, 2, 4],
 }
-ORDER = ["publish_lazy", "max_inflight_roots", "warps_per_sm", "block", "steal_batch", "deque_capacity", "probe_width",
+ORDER = ["publish_lazy", "max_inflight_roots", "leaf_batch", "warps_per_sm", "block", "steal_batch", "deque_capacity", "probe_width",
          "victim_policy", "num_queues", "spawn_capacity"]
 
 
@@ -190,7 +193,7 @@ def run(workload="mix", reps=3, sweeps=2, n_roots=None, out=None, quiet=False, s
              "steal_batch": defaults.steal_batch, "probe_width": defaults.probe_width,
              "victim_policy": defaults.victim_policy, "num_queues": defaults.num_queues,
              "spawn_capacity": defaults.spawn_capacity, "max_inflight_roots": defaults.max_inflight_roots,
-             "publish_lazy": defaults.publish_lazy}
+             "publish_lazy": defaults.publish_lazy, "leaf_batch": defaults.leaf_batch}
     start.update(start_point or {})
     t0 = time.time()
     best, best_t, trials = coordinate_descent(measure, start, sweeps=sweeps, log=log)

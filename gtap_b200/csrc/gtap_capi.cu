@@ -46,6 +46,7 @@ struct Runtime {
     int workers_full = 0;       // thread_worker_kernel<BuiltinProgram>
     int workers_light = 0;      // thread_worker_kernel_lb<BuiltinProgramLight>
     bool fibnq_ok = false;      // thread_worker_kernel_lb<BuiltinProgramFibNq> fits as many workers
+    bool stage_light = false;   // g.smem_bytes holds a record stage per warp
     int workers_block = 0;      // block_worker_kernel<BlockProgram>: one worker per block (block mode only)
     int last_workers = 0;       // workers of the last launch
     bool last_block = false;    // the last launch ran the block kernel
@@ -161,7 +162,9 @@ bool roots_need_sorts(const gtap_root* roots, int n) {
 }
 
 // layouts the Python binding and other FFI callers mirror
-static_assert(sizeof(gtap_config) == 88 && offsetof(gtap_config, admit_order) == 80, "gtap_config layout");
+static_assert(sizeof(gtap_config) == 88 && offsetof(gtap_config, admit_order) == 80 &&
+                  offsetof(gtap_config, leaf_batch) == 84,
+              "gtap_config layout");
 static_assert(sizeof(gtap_run_stats) == 168 && offsetof(gtap_run_stats, light_kernel_ms) == 160,
               "gtap_run_stats layout");
 static_assert(sizeof(gtap_root) == 56 && sizeof(gtap_root_result) == 40, "root layouts");
@@ -353,6 +356,9 @@ Arena make_arena(int n_roots, int mode, int workers, int first_root = 0) {
     A.handle_cap = c.result_handles;
     A.staging = g.staging;
     A.leaf_buf = g.leaf_buf;
+    // the kernels this arena launches hold a record stage per warp (the light
+    // kernels in g.smem_bytes, the sorting kernel in its leaf buffers)
+    A.rec_prefetch = g.stage_light ? 1 : 0;
     return A;
 }
 
@@ -392,6 +398,7 @@ int validate_config(const gtap_config& c) {
     if (c.profile_samples < 0 || c.result_handles < 1) return GTAP_ERROR_INVALID_ARGUMENT;
     if (c.publish_lazy < 0 || c.publish_lazy > 1 || c.max_inflight_roots < 0) return GTAP_ERROR_INVALID_ARGUMENT;
     if (c.admit_order < GTAP_ADMIT_AS_GIVEN || c.admit_order > GTAP_ADMIT_SPLIT) return GTAP_ERROR_INVALID_ARGUMENT;
+    if (c.leaf_batch < 0 || c.leaf_batch > 8) return GTAP_ERROR_INVALID_ARGUMENT;
     return 0;
 }
 
@@ -470,6 +477,7 @@ int launch_resident(int n_roots, cudaStream_t s, float* ms_out, bool light, int 
     g.last_block = block_mode();
     Arena A = make_arena(n_roots, 0, W, first_root);
     if (rec_stride > 0 && rec_stride < A.rec_stride) A.rec_stride = rec_stride;
+    if (!light && !block_mode()) A.rec_prefetch = g.leaf_buf > 0 ? 1 : 0;   // the sorting kernel: its leaf buffers
     const int fresh_base = W * g.cfg.ids_per_worker;
     A.admit_watermark = admission_watermark(W);
     reset_kernel<<<std::max(1, std::min(1184, (std::max(n_roots, W * g.cfg.num_queues) + 255) / 256)), 256, 0,
@@ -576,9 +584,12 @@ int run_batch(const gtap_root* roots, int n_roots, gtap_root_result* results, gt
         segs.push_back({0, n_roots, !sorts});
     } else if (halves) {
         const int a = (n_light + 1) / 2;
-        segs = {{0, a, true}, {n_light, n_roots - n_light, false}, {a, n_light - a, true}};
+        segs.push_back({0, a, true});
+        segs.push_back({n_light, n_roots - n_light, false});
+        segs.push_back({a, n_light - a, true});
     } else {
-        segs = {{0, n_light, true}, {n_light, n_roots - n_light, false}};
+        segs.push_back({0, n_light, true});
+        segs.push_back({n_light, n_roots - n_light, false});
     }
 
     double ms_total = 0, ms_light = 0;
@@ -681,6 +692,7 @@ int gtap_default_config(gtap_config* cfg) {
     cfg->publish_lazy = 0;
     cfg->max_inflight_roots = 0;
     cfg->admit_order = GTAP_ADMIT_SPLIT;
+    cfg->leaf_batch = 1;
     return 0;
 }
 
@@ -697,12 +709,17 @@ static int initialize_impl(const gtap_config* cfg_in, int external_workers) {
     GT_CUDA(cudaGetDevice(&g.device));
     GT_CUDA(cudaDeviceGetAttribute(&g.sm_count, cudaDevAttrMultiProcessorCount, g.device));
     const size_t smem = smem_for(c);
-    // the sorting kernel also holds leaf buffers: per warp kLeafBatch input
-    // buffers and an output buffer, or fewer inputs when the block's shared
-    // memory cannot hold them
     int smem_optin = 0;
     GT_CUDA(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, g.device));
-    int leaf_buf = prog::kLeafBatch;
+    // the light kernels also hold a record stage per warp (16 bytes of slack
+    // to align it), when the block's shared memory can hold it
+    size_t smem_light = smem + (size_t)(c.block / 32) * (kRecStageBytes + 16);
+    const bool stage_light = smem_light <= (size_t)smem_optin;
+    if (!stage_light) smem_light = smem;
+    // the sorting kernel also holds leaf buffers: per warp leaf_batch input
+    // buffers and an output buffer, or fewer inputs when the block's shared
+    // memory cannot hold them
+    int leaf_buf = c.leaf_batch > 0 ? c.leaf_batch : 1;
     size_t smem_full = smem;
     for (; leaf_buf > 0; leaf_buf /= 2) {
         smem_full = smem + (size_t)(c.block / 32) * (leaf_buf + 1) * BuiltinProgram::kLeafKeys * sizeof(int);
@@ -711,15 +728,18 @@ static int initialize_impl(const gtap_config* cfg_in, int external_workers) {
     if (leaf_buf == 0) smem_full = smem;
     int per_sm_full = 0, per_sm_light = 0;
     GT_CUDA(cudaFuncSetAttribute(kernel_full(c.num_queues), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_full));
-    GT_CUDA(cudaFuncSetAttribute(kernel_light(c.num_queues), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    GT_CUDA(cudaFuncSetAttribute(kernel_light(c.num_queues), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem_light));
     if (c.block <= kFullKernelThreads)   // the sorting kernel's launch bound
         GT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_full, kernel_full(c.num_queues), c.block, smem_full));
-    GT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_light, kernel_light(c.num_queues), c.block, smem));
+    GT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_light, kernel_light(c.num_queues), c.block, smem_light));
     if (per_sm_light < 1) return GTAP_ERROR_INVALID_ARGUMENT;
     {
         int per_sm_fibnq = 0;
-        GT_CUDA(cudaFuncSetAttribute(kernel_fibnq(c.num_queues), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        GT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_fibnq, kernel_fibnq(c.num_queues), c.block, smem));
+        GT_CUDA(cudaFuncSetAttribute(kernel_fibnq(c.num_queues), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem_light));
+        GT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_fibnq, kernel_fibnq(c.num_queues), c.block,
+                                                              smem_light));
         g.fibnq_ok = per_sm_fibnq >= per_sm_light;
     }
     // one resident wave per variant; grid = 0 fills the GPU, otherwise cap it
@@ -753,7 +773,8 @@ static int initialize_impl(const gtap_config* cfg_in, int external_workers) {
         if (c.ids_per_worker < 64) return GTAP_ERROR_INVALID_ARGUMENT;
     }
     g.cfg = c;
-    g.smem_bytes = smem;
+    g.smem_bytes = smem_light;
+    g.stage_light = stage_light;
     g.smem_full = smem_full;
     g.leaf_buf = leaf_buf;
 

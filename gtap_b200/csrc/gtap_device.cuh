@@ -116,6 +116,14 @@ __device__ __forceinline__ int4 ld_cg_v4(const void* p) {
 #ifndef GTAP_RECORD_LOAD
 #define GTAP_RECORD_LOAD 1
 #endif
+// 16-byte asynchronous copy global -> shared through L2 (the path of ld.cg);
+// both addresses 16-byte aligned.  rec_stage_wait: this thread's copies done.
+__device__ __forceinline__ void cp_async16_cg(void* smem_dst, const void* gmem_src) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void rec_stage_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 __device__ __forceinline__ int4 ld_data_v4(const void* p) {
 #if GTAP_RECORD_LOAD == 0
     int4 v;
@@ -353,6 +361,8 @@ struct Arena {
     int* staging;
     int handle_cap;
     int leaf_buf;                      // leaf input buffers per warp at the end of dynamic shared memory (0: none)
+    int rec_prefetch;                  // 1: the kernel's dynamic shared memory holds a record stage per warp
+                                       //    (kRecStageBytes; the leaf buffers double as it where there are any)
 };
 
 // ---------------------------------------------------------------------------

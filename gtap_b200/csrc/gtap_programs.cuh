@@ -294,7 +294,8 @@ static __device__ __noinline__ void warp_merge(const int* a, int alen, const int
 }
 
 // Leaves of at most kLeafKeys keys go through the warp's shared-memory leaf
-// buffers: kLeafBatch input buffers of kLeafKeys keys and one output buffer.
+// buffers: gtap_config.leaf_batch input buffers of kLeafKeys keys and one
+// output buffer.
 // The keys of a batch of leaves are copied in with cp.async (every copy of
 // every leaf of the batch in flight at once: one round trip per batch, no
 // registers held), merge-path searches and merges read shared memory, and
@@ -304,10 +305,6 @@ static __device__ __noinline__ void warp_merge(const int* a, int alen, const int
 // stay rolled: the mix runs these leaves beside fib and n-queens tasks on the
 // same SMs, which share the instruction cache with them.
 constexpr int kLeafKeys = 256;
-// Input buffers per warp.  Batches of four leaves measured no faster than
-// one leaf at a time, and their shared memory limits how many workers fit an
-// SM: one input buffer and the output buffer, 2 KB per warp.
-constexpr int kLeafBatch = 1;
 
 __device__ __forceinline__ void cp_async4(int* smem_dst, const int* gmem_src) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);

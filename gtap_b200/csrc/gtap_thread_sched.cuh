@@ -61,6 +61,9 @@ constexpr int kFreedCap = 96;
 constexpr int kRootBalCap = 8;
 constexpr int kBalChunk = 1024;
 constexpr int kLocalCap = 128;     // per-warp, per-queue local ready stack (power of two)
+// Per-warp record stage: each lane's next task record (header and up to 32
+// frame bytes), copied in while the previous round ends.
+constexpr int kRecStageBytes = kWarp * 48;
 constexpr int kReserve = 32;       // ready tasks a warp keeps when others are hungry
 constexpr int kHungryReplicas = 8;  // copies of the hungry-worker count, 128 bytes apart
 constexpr int kHungryStride = 32;
@@ -104,6 +107,7 @@ struct WarpShared {
     int* sbuf;                 // [num_queues][spawn_cap] staged child ids (| spawner lane << 27)
     int* lstk;                 // [num_queues][kLocalCap] ready tasks not yet visible to thieves
     int* lbuf;                 // leaf buffers: [A.leaf_buf + 1][Prog::kLeafKeys] (programs with warp leaves), or null
+    int4* rstage;              // record stage [kWarp][3] (kRecStageBytes), or null: records are loaded when a round starts
 };
 
 // Positions of this warp's local stacks and deques.  Only the scheduler
@@ -881,6 +885,7 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
         return now - S.t_watch > A.watchdog_ns;
     };
     int round = 0;
+    bool staged = false;                     // this round's records are in S.rstage (copies in flight)
     int src_kind = 0;                        // debug builds: where this round's tasks came from
     bool idle = false;                       // counted in the hungry replicas
     unsigned long long idle_since = 0;       // lane 0: start of the current idle stretch
@@ -974,17 +979,28 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
         int4 hw = make_int4(0, -1, 0, 0), fw0 = make_int4(0, 0, 0, 0), fw1 = fw0;
         unsigned long long fn = 0;
         int bad = 0;
+        if (staged) rec_stage_wait();
         if ((int)lane < nb) {
             if ((unsigned)my_tid >= (unsigned)A.total_ids) {
                 bad = 1;
             } else {
                 // header, the first 32 frame bytes and (programs that call
-                // through a function table) the task function, in one round trip
+                // through a function table) the task function, in one round
+                // trip, or from the record stage the previous round filled
                 const char* rec = A.records + (size_t)my_tid * A.rec_stride;
-                hw = ld_data_v4(rec);
-                if (Prog::kFrameWords) {
-                    fw0 = ld_data_v4(rec + 16);
-                    if (A.rec_stride >= 48) fw1 = ld_data_v4(rec + 32);
+                if (staged) {
+                    const int4* st4 = S.rstage + lane * 3;
+                    hw = st4[0];
+                    if (Prog::kFrameWords) {
+                        fw0 = st4[1];
+                        if (A.rec_stride >= 48) fw1 = st4[2];
+                    }
+                } else {
+                    hw = ld_data_v4(rec);
+                    if (Prog::kFrameWords) {
+                        fw0 = ld_data_v4(rec + 16);
+                        if (A.rec_stride >= 48) fw1 = ld_data_v4(rec + 32);
+                    }
                 }
                 if (Prog::kFuncTable) fn = ld_data_u64(reinterpret_cast<const unsigned long long*>(A.funcs) + my_tid);
                 if ((unsigned)hw.w >= (unsigned)A.n_roots || hw.y < -1 || hw.y >= A.total_ids) bad = 2;
@@ -1207,6 +1223,26 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
                 }
             }
         }
+        // the next batch's records (children this warp wrote, parents this
+        // warp resumed) start on their way to the record stage: the copies
+        // overlap the rest of the round end.  No other warp can take these
+        // tasks any more, and this warp wrote or acquired their records: the
+        // warp barrier orders every lane's stores before the copies, as it
+        // orders them before the loads of a round that starts unstaged.
+        staged = false;
+        if (nb_next > 0 && S.rstage != nullptr) {
+            __syncwarp();
+            if ((int)lane < nb_next && (unsigned)next_tid < (unsigned)A.total_ids) {
+                const char* rec = A.records + (size_t)next_tid * A.rec_stride;
+                int4* st4 = S.rstage + lane * 3;
+                cp_async16_cg(st4, rec);
+                if (Prog::kFrameWords) {
+                    cp_async16_cg(st4 + 1, rec + 16);
+                    if (A.rec_stride >= 48) cp_async16_cg(st4 + 2, rec + 32);
+                }
+            }
+            staged = true;
+        }
         // (5) publication of the deque entries staged above (its own fence:
         //     the slot stores, and the records when nothing joined)
         publish_commit(A, S, P, false);
@@ -1281,6 +1317,7 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
             if (__shfl_sync(0xffffffffu, stop, 0)) break;
         }
     }
+    rec_stage_wait();   // no copy outlives the loop
     if (lane == 0) flush_all_bal(A, S);
 }
 
@@ -1290,13 +1327,14 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
 // created before the loop, e.g. by the drop-in __gtap_push_initial_task).
 template <class Prog, int QM>
 __device__ __forceinline__ void thread_worker_run(const Arena& A, WarpShared& S, int worker, int* sbuf, int* lstk,
-                                                  int initial_tid, int* lbuf = nullptr) {
+                                                  int initial_tid, int* lbuf = nullptr, int4* rstage = nullptr) {
     const unsigned lane = lane_id();
     if (lane == 0) {
         S.worker = worker;
         S.sbuf = sbuf;
         S.lstk = lstk;
         S.lbuf = lbuf;
+        S.rstage = rstage;
         for (int k = 0; k < kMaxQueues; ++k) S.cnt[k] = 0;
         S.alloc_last = 0;
         S.alloc_pos = 0;
@@ -1323,7 +1361,11 @@ __device__ __forceinline__ void thread_worker_run(const Arena& A, WarpShared& S,
 }
 
 // Kernel body: warps_per_block WarpShared records + staging buffers in dynamic
-// smem, then (programs with warp leaves) A.leaf_buf + 1 leaf buffers per warp.
+// smem, then (programs with warp leaves) A.leaf_buf + 1 leaf buffers per warp,
+// or (A.rec_prefetch, programs without them) a record stage of
+// kRecStageBytes + 16 per warp.  The leaf buffers (2 KB or more a warp) double
+// as the record stage: the stage is filled at a round's end and read when the
+// next round starts, the leaf buffers only in between.
 template <class Prog, int QM>
 __device__ __forceinline__ void thread_worker_body(const Arena& A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1332,11 +1374,17 @@ __device__ __forceinline__ void thread_worker_body(const Arena& A) {
     int* sb_base = reinterpret_cast<int*>(smem_raw + sizeof(WarpShared) * A.warps_per_block);
     int* ls_base = sb_base + (size_t)A.warps_per_block * A.num_queues * A.spawn_cap;
     int* lb_base = ls_base + (size_t)A.warps_per_block * A.num_queues * kLocalCap;
+    const bool leaves = Prog::kLeafKeys && A.leaf_buf;
+    int* lbuf = leaves ? lb_base + (size_t)wib * (A.leaf_buf + 1) * Prog::kLeafKeys : nullptr;
+    int4* rstage = nullptr;
+    if (A.rec_prefetch) {
+        char* st = leaves ? reinterpret_cast<char*>(lbuf)
+                          : reinterpret_cast<char*>(lb_base) + (size_t)wib * (kRecStageBytes + 16);
+        rstage = reinterpret_cast<int4*>((reinterpret_cast<uintptr_t>(st) + 15) & ~(uintptr_t)15);
+    }
     thread_worker_run<Prog, QM>(A, ws[wib], blockIdx.x * A.warps_per_block + wib,
                             sb_base + (size_t)wib * A.num_queues * A.spawn_cap,
-                            ls_base + (size_t)wib * A.num_queues * kLocalCap, -1,
-                            (Prog::kLeafKeys && A.leaf_buf) ? lb_base + (size_t)wib * (A.leaf_buf + 1) * Prog::kLeafKeys
-                                                            : nullptr);
+                            ls_base + (size_t)wib * A.num_queues * kLocalCap, -1, lbuf, rstage);
 }
 
 

@@ -88,6 +88,9 @@ typedef struct gtap_config {
                                 1: keep up to 128 ready tasks per queue private until some worker is idle */
     int32_t max_inflight_roots; /* roots admitted but not finished, at most; 0 = no limit */
     int32_t admit_order;     /* GTAP_ADMIT_*: the order in which a batch launch admits its roots */
+    int32_t leaf_batch;      /* sort-capable kernel: sort and merge leaves a warp stages in shared memory
+                                at once, 1..8, 0 = 1 (one load round trip per batch; each costs 1 KB per
+                                warp of shared memory) */
 } gtap_config;
 
 /* Admission order of a batch (gtap_launch, gtap_run_host).  Results come back

@@ -45,7 +45,7 @@ def test_struct_layouts_match_header():
     assert ctypes.sizeof(gt.RootResult) == 40
     assert ctypes.sizeof(gt.Config) == 88
     assert gt.Config.total_ids.offset == 40
-    assert gt.Config.admit_order.offset == 80
+    assert gt.Config.admit_order.offset == 80 and gt.Config.leaf_batch.offset == 84
     assert ctypes.sizeof(gt.RunStats) == 168
     assert gt.RunStats.light_kernel_ms.offset == 160
 
