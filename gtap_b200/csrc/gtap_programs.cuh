@@ -302,8 +302,11 @@ static __device__ __noinline__ void warp_merge(const int* a, int alen, const int
 // results leave with coalesced stores.  A merge leaf done in
 // global memory costs a dependent round trip per binary-search step and per
 // merged key, and leaves done one at a time a round trip each.  The loops
-// stay rolled: the mix runs these leaves beside fib and n-queens tasks on the
-// same SMs, which share the instruction cache with them.
+// stay rolled and the two leaf routines inline: unrolled loops measured
+// slower even with the sort kernel alone on the SMs (the instruction cache
+// again), and calls out of line slower than inlined code (the 2^10-2^20-key
+// cilksort roots of the seed-42 mix: 26.7 ms out of line, 25.0 ms inline,
+// 28.1 ms inline and unrolled).
 constexpr int kLeafKeys = 256;
 
 __device__ __forceinline__ void cp_async4(int* smem_dst, const int* gmem_src) {
@@ -344,7 +347,7 @@ __device__ __forceinline__ void leaf_store(const int* buf, int total, int* dst) 
 
 // in = a[0, alen) ++ b[0, blen), both sorted: dst[0, alen + blen) = their
 // merge (the sequence warp_merge writes), through out.
-static __device__ __noinline__ void leaf_merge_out(const int* in, int alen, int blen, int* out, int* dst) {
+__device__ __forceinline__ void leaf_merge_out(const int* in, int alen, int blen, int* out, int* dst) {
     __syncwarp();   // out's previous contents were stored already
     const int d0 = (int)lane_id() * 8;
     if (d0 < alen + blen) merge_path8(in, alen, in + alen, blen, d0, out);
@@ -354,7 +357,7 @@ static __device__ __noinline__ void leaf_merge_out(const int* in, int alen, int 
 
 // dst[0, n) = in[0, n) sorted: 64-key runs sorted in place by
 // warp_bitonic64, then merge passes of doubling width between in and out.
-static __device__ __noinline__ void leaf_sort_out(int* in, int n, int* out, int* dst) {
+__device__ __forceinline__ void leaf_sort_out(int* in, int n, int* out, int* dst) {
     const int lane = (int)lane_id();
     __syncwarp();   // out's previous contents were stored already
 #pragma unroll 1
@@ -775,7 +778,9 @@ __device__ __forceinline__ void treesum_task(const Arena& A, WarpShared& S, void
 // kSorts = false leaves the register-heavy sorting kinds out of the kernel,
 // which lets fib / n-queens / BFS / tree launches run at higher occupancy;
 // kGraphs = false also leaves out BFS and tree sums, so that a launch of fib
-// and n-queens roots runs a kernel with two task bodies.
+// and n-queens roots runs a kernel with two task bodies.  A task of a kind
+// left out is recorded as ERR_INVALID_KIND.  (A sorting kernel without the
+// fib, n-queens, BFS and tree bodies measured no faster on sort roots alone.)
 template <bool kSorts, bool kGraphs = true>
 struct BuiltinProgramT {
     static constexpr int kFrameBytes = prog::kFrameBytes;
