@@ -55,7 +55,7 @@ namespace gtap {
 #define GTAP_PHASE_ADD(slot, t0, t1) (void)0
 #endif
 
-constexpr int kAvailCap = 256;    // per-warp cache of free task ids
+constexpr int kAvailCap = 256;    // per-warp cache of free task ids (a ring; power of two)
 constexpr int kAvailHigh = 240;   // above this, 32 ids go back to the recycled pool
 constexpr int kFreedCap = 96;
 constexpr int kRootBalCap = 8;
@@ -94,6 +94,7 @@ struct WarpShared {
     int l_pend[kWarp];         // detached child past the staging buffer whose frame is still being written (-1: none)
     int cnt[kMaxQueues];       // children staged this round, per queue
     int avail_n, alloc_pos, freed_n, bump;
+    int avail_head;            // avail[] is a ring: the next free id is avail[avail_head]
     int alloc_last;            // ids this warp allocated last round (refill target)
     int avail[kAvailCap];
     int freed[kFreedCap];
@@ -208,38 +209,31 @@ __device__ __forceinline__ int warp_agg_inc(int* p, unsigned m) {
 
 __device__ __forceinline__ int alloc_id(const Arena& A, WarpShared& S) {
     const int a = warp_agg_inc(&S.alloc_pos, __activemask());
-    if (a < S.avail_n) return S.avail[a];
+    if (a < S.avail_n) return S.avail[(S.avail_head + a) & (kAvailCap - 1)];
     return alloc_id_slow(A, S);
 }
 
-// Warp-cooperative: compact the cache after a round, return surplus ids to
-// the global ring and refill from the private range / ring / fresh ids.
+// Warp-cooperative, after a round: drop the ids the round took from the
+// front of the cache ring, append the ids it freed, return surplus ids to the
+// global ring and refill from the private range / ring / fresh ids.
 static __device__ void id_cache_maintain(const Arena& A, WarpShared& S) {
     const unsigned lane = lane_id();
     __syncwarp();
-    int consumed = min(S.alloc_pos, S.avail_n);
-    int remain = S.avail_n - consumed;
-    int nfreed = min(S.freed_n, kFreedCap);
+    const int consumed = min(S.alloc_pos, S.avail_n);
+    const int head = (S.avail_head + consumed) & (kAvailCap - 1);
+    int n = S.avail_n - consumed;   // cached ids, avail[head], avail[head + 1], ...
+    const int nfreed = min(S.freed_n, kFreedCap);
     const int used_this_round = S.alloc_pos;
-    // move remaining entries to the front (read all, then write)
-    int v[kAvailCap / 32];
-#pragma unroll
-    for (int j = 0; j < kAvailCap / 32; ++j)
-        v[j] = ((int)lane + 32 * j < remain) ? S.avail[consumed + lane + 32 * j] : 0;
-    __syncwarp();
-#pragma unroll
-    for (int j = 0; j < kAvailCap / 32; ++j)
-        if ((int)lane + 32 * j < remain) S.avail[lane + 32 * j] = v[j];
-    __syncwarp();
+    int* const ring = S.avail;
+    auto at = [&](int i) -> int& { return ring[(head + i) & (kAvailCap - 1)]; };
     // append freed ids; whatever does not fit goes to the global ring
-    int n = remain;
     for (int base = 0; base < nfreed; base += 32) {
         int i = base + (int)lane;
         int id = (i < nfreed) ? S.freed[i] : -1;
         int take = min(32, nfreed - base);
         int room = kAvailCap - n;
         if (take <= room) {
-            if ((int)lane < take) S.avail[n + lane] = id;
+            if ((int)lane < take) at(n + (int)lane) = id;
             n += take;
         } else {
             // push this chunk of freed ids to the recycled-id ring
@@ -247,9 +241,9 @@ static __device__ void id_cache_maintain(const Arena& A, WarpShared& S) {
         }
         __syncwarp();
     }
-    // surplus: give 32 back
+    // surplus: give the 32 newest back
     if (n > min(kAvailHigh, A.avail_target + 32)) {
-        int id = S.avail[n - 32 + lane];
+        int id = at(n - 32 + (int)lane);
         __syncwarp();
         ring_push_warp(A, A.idpool, id, 32);
         n -= 32;
@@ -262,7 +256,7 @@ static __device__ void id_cache_maintain(const Arena& A, WarpShared& S) {
         int b = S.bump;
         if (b < A.ids_per_worker) {
             int k = min(32, A.ids_per_worker - b);
-            if ((int)lane < k) S.avail[n + lane] = A.id_base + S.worker * A.ids_per_worker + b + lane;
+            if ((int)lane < k) at(n + (int)lane) = A.id_base + S.worker * A.ids_per_worker + b + lane;
             got = k;
             __syncwarp();
             if (lane == 0) S.bump = b + k;
@@ -270,7 +264,7 @@ static __device__ void id_cache_maintain(const Arena& A, WarpShared& S) {
         if (got == 0) {
             int id = -1;
             got = ring_pop_warp(A, A.idpool, 32, &id, true);
-            if ((int)lane < got) S.avail[n + lane] = id;
+            if ((int)lane < got) at(n + (int)lane) = id;
         }
         if (got == 0) {
             unsigned f = 0;
@@ -278,7 +272,7 @@ static __device__ void id_cache_maintain(const Arena& A, WarpShared& S) {
             f = __shfl_sync(0xffffffffu, f, 0);
             if (f < (unsigned)A.total_ids) {
                 int k = min(32, A.total_ids - (int)f);
-                if ((int)lane < k) S.avail[n + lane] = (int)f + lane;
+                if ((int)lane < k) at(n + (int)lane) = (int)f + lane;
                 got = k;
             }
         }
@@ -288,6 +282,7 @@ static __device__ void id_cache_maintain(const Arena& A, WarpShared& S) {
     }
     __syncwarp();
     if (lane == 0) {
+        S.avail_head = head;
         S.avail_n = n;
         S.alloc_pos = 0;
         S.freed_n = 0;
@@ -1351,6 +1346,7 @@ __device__ __forceinline__ void thread_worker_run(const Arena& A, WarpShared& S,
     if ((int)lane < first) S.avail[lane] = range + (int)lane;
     if ((int)lane + 32 < first) S.avail[lane + 32] = range + (int)lane + 32;
     if (lane == 0) {
+        S.avail_head = 0;
         S.avail_n = first;
         S.bump = first;
     }
