@@ -20,7 +20,8 @@ Search: coordinate descent from the library defaults over
                  (one load round trip per batch, 1 KB of shared memory each)
   publish_lazy   0: publish every ready task beyond the next batch each round;
                  1: keep up to a batch in reserve privately until some worker is
-                 idle (fuller rounds once the GPU is busy, a slower ramp-up)
+                 idle (fuller rounds once the GPU is busy, a slower ramp-up);
+                 2: 1 without sort leaves, 0 in the sorting kernel
   max_inflight_roots  roots admitted and not finished, at most (0: no limit);
                  an asynchronous BFS relaxes vertices more than once the more
                  roots share the GPU, so served batches of BFS roots do less
@@ -58,7 +59,7 @@ SPACE = {
     "num_queues": [1, 2, 4],
     "spawn_capacity": [128, 256, 512, 1024],
     "max_inflight_roots": [0, 8, 16, 32, 64, 128],
-    "publish_lazy": [0, 1],
+    "publish_lazy": [0, 1, 2],
     "leaf_batch": [1, 2, 4],
 }
 ORDER = ["publish_lazy", "max_inflight_roots", "leaf_batch", "warps_per_sm", "block", "steal_batch", "deque_capacity", "probe_width",

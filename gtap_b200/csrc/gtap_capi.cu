@@ -308,7 +308,7 @@ Arena make_arena(int n_roots, int mode, int workers, int first_root = 0) {
     A.rec_stride = kHdrBytes + ((c.frame_bytes + 15) / 16) * 16;
     A.admit_batch = c.admit_batch;
     A.mode = mode;
-    A.publish_lazy = c.publish_lazy;
+    A.publish_lazy = c.publish_lazy != 0 ? 1 : 0;
     A.max_inflight = c.max_inflight_roots;
     A.total_ids = (int)c.total_ids;
     A.watchdog_ns = (unsigned long long)c.watchdog_ms * 1000000ull;
@@ -396,7 +396,7 @@ int validate_config(const gtap_config& c) {
     if (c.admit_batch < 1 || c.admit_batch > 32) return GTAP_ERROR_INVALID_ARGUMENT;
     if (c.watchdog_ms < 1) return GTAP_ERROR_INVALID_ARGUMENT;
     if (c.profile_samples < 0 || c.result_handles < 1) return GTAP_ERROR_INVALID_ARGUMENT;
-    if (c.publish_lazy < 0 || c.publish_lazy > 1 || c.max_inflight_roots < 0) return GTAP_ERROR_INVALID_ARGUMENT;
+    if (c.publish_lazy < 0 || c.publish_lazy > 2 || c.max_inflight_roots < 0) return GTAP_ERROR_INVALID_ARGUMENT;
     if (c.admit_order < GTAP_ADMIT_AS_GIVEN || c.admit_order > GTAP_ADMIT_SPLIT) return GTAP_ERROR_INVALID_ARGUMENT;
     if (c.leaf_batch < 0 || c.leaf_batch > 8) return GTAP_ERROR_INVALID_ARGUMENT;
     return 0;
@@ -477,7 +477,10 @@ int launch_resident(int n_roots, cudaStream_t s, float* ms_out, bool light, int 
     g.last_block = block_mode();
     Arena A = make_arena(n_roots, 0, W, first_root);
     if (rec_stride > 0 && rec_stride < A.rec_stride) A.rec_stride = rec_stride;
-    if (!light && !block_mode()) A.rec_prefetch = g.leaf_buf > 0 ? 1 : 0;   // the sorting kernel: its leaf buffers
+    if (!light && !block_mode()) {
+        A.rec_prefetch = g.leaf_buf > 0 ? 1 : 0;   // the sorting kernel: its leaf buffers
+        if (g.cfg.publish_lazy == 2) A.publish_lazy = 0;
+    }
     const int fresh_base = W * g.cfg.ids_per_worker;
     A.admit_watermark = admission_watermark(W);
     reset_kernel<<<std::max(1, std::min(1184, (std::max(n_roots, W * g.cfg.num_queues) + 255) / 256)), 256, 0,

@@ -294,7 +294,7 @@ struct Arena {
     int admit_batch;        // roots claimed per admission
     int mode;               // GTAP_MODE_*
     int id_base;            // first id of the private ranges (ids below it are reserved)
-    int publish_lazy;       // see gtap_config::publish_lazy
+    int publish_lazy;       // 0 or 1 for this launch (gtap_config::publish_lazy)
     int max_inflight;       // admitted-but-unfinished roots allowed (0 = unlimited)
     int total_ids;          // ids in the arena
     unsigned long long watchdog_ns;

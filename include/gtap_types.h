@@ -85,7 +85,9 @@ typedef struct gtap_config {
     int32_t profile_samples; /* per-worker timeline samples, 0 = off (MAX_PROFILE_DATA) */
     int32_t result_handles;  /* legacy result-handle table capacity (GTAP_RESULT_HANDLE_CAPACITY) */
     int32_t publish_lazy;    /* 0: publish every task beyond the next batch each round (reference push_batch);
-                                1: keep up to 128 ready tasks per queue private until some worker is idle */
+                                1: keep up to 128 ready tasks per queue private until some worker is idle;
+                                2: 1 in launches without sort leaves, 0 in the sorting kernel (whose long
+                                   rounds leave idle workers waiting for a private reserve) */
     int32_t max_inflight_roots; /* roots admitted but not finished, at most; 0 = no limit */
     int32_t admit_order;     /* GTAP_ADMIT_*: the order in which a batch launch admits its roots */
     int32_t leaf_batch;      /* sort-capable kernel: sort and merge leaves a warp stages in shared memory
