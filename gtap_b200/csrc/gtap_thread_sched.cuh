@@ -1100,15 +1100,13 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
             }
             __syncwarp();
         }
-        // (2) one warp-wide fence orders this round's stores (children's
-        //     records, results written into parents' frames, orphan marks)
-        //     before the join decrements, which therefore need only acquire
-        //     semantics.
-        const unsigned joiners = __ballot_sync(0xffffffffu, my_fin && S.l_parent[lane] >= 0);
-        if (joiners) {
-            fence_acq_rel();
-            __syncwarp();
-        }
+        // (2) no fence before the joins: each join decrement is an
+        //     acquire-release atomic, which releases the results the lane
+        //     wrote into its parent's frame and, through this warp barrier,
+        //     the stores of the other lanes before it.  Leaf data is fenced
+        //     after the leaf work; orphan marks and children's records reach
+        //     other warps only through publication, which has its own fence.
+        __syncwarp();
         GTAP_PHASE_MARK(ph3);
         GTAP_PHASE_ADD(12, ph2, ph3);
         // (3) joins: the last child re-enqueues its parent on the resume queue;
@@ -1117,7 +1115,7 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
         if (my_fin) {
             const int parent = S.l_parent[lane];
             if (parent >= 0) {
-                const int old = atom_add_acquire(&hdr_of(A, parent)->join, -1);
+                const int old = atom_add_acq_rel(&hdr_of(A, parent)->join, -1);
                 if ((old & kJoinCountMask) == 1) {
                     rq = (old >> 24) & 7;
                     if (rq >= A.num_queues) rq = 0;
