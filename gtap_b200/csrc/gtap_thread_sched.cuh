@@ -705,7 +705,7 @@ static __device__ void publish_stage(const Arena& A, WarpShared& S, QueuePos<QM>
 // One warp-wide fence orders every store this warp made so far (task
 // records, results, deque slots) before what follows; then lane 0 moves the
 // bottoms of the deques publish_stage wrote, making those entries stealable.
-// fence: also when nothing is pending (the joins that follow rely on it).
+// fence: also when nothing is pending.
 template <int QM>
 static __device__ void publish_commit(const Arena& A, WarpShared& S, QueuePos<QM>& P, bool fence) {
     const unsigned lane = lane_id();
