@@ -8,8 +8,8 @@ and cutoffs 64/256) in one batch call (gtap_launch): admitted grouped by kind
 and run as two persistent launches, the fib and n-queens roots and then the
 cilksort roots.  Metric: tasks/s (spawned tasks, root included).  Inputs are
 resident in HBM when the timed region starts; the key slabs (~2.6 GB) exceed
-L2, and each step's cilksort leaves
-read the pristine input, so no restore happens between steps.
+L2, and each step's cilksort leaves read the pristine input, so no restore
+happens between steps.
 
 Prints ONE JSON line (rank 0).  --impl reference times the reference's
 sequential programs (CPU, the oracle's restatement of seq_fib.c / seq_nq.c /
