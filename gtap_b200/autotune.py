@@ -22,6 +22,8 @@ Search: coordinate descent from the library defaults over
                  1: keep up to a batch in reserve privately until some worker is
                  idle (fuller rounds once the GPU is busy, a slower ramp-up);
                  2: 1 without sort leaves, 0 in the sorting kernel
+  join_walk      rounds of at most this many tasks run fib's sums at their joins
+                 (0: never); the tree's drain gains, full rounds would wait
   max_inflight_roots  roots admitted and not finished, at most (0: no limit);
                  an asynchronous BFS relaxes vertices more than once the more
                  roots share the GPU, so served batches of BFS roots do less
@@ -61,9 +63,10 @@ SPACE = {
     "max_inflight_roots": [0, 8, 16, 32, 64, 128],
     "publish_lazy": [0, 1, 2],
     "leaf_batch": [1, 2, 4],
+    "join_walk": [0, 2, 4, 8, 32],
 }
 ORDER = ["publish_lazy", "max_inflight_roots", "leaf_batch", "warps_per_sm", "block", "steal_batch", "deque_capacity", "probe_width",
-         "victim_policy", "num_queues", "spawn_capacity"]
+         "victim_policy", "num_queues", "spawn_capacity", "join_walk"]
 
 
 def to_overrides(point, sm_count):
@@ -194,7 +197,8 @@ def run(workload="mix", reps=3, sweeps=2, n_roots=None, out=None, quiet=False, s
              "steal_batch": defaults.steal_batch, "probe_width": defaults.probe_width,
              "victim_policy": defaults.victim_policy, "num_queues": defaults.num_queues,
              "spawn_capacity": defaults.spawn_capacity, "max_inflight_roots": defaults.max_inflight_roots,
-             "publish_lazy": defaults.publish_lazy, "leaf_batch": defaults.leaf_batch}
+             "publish_lazy": defaults.publish_lazy, "leaf_batch": defaults.leaf_batch,
+             "join_walk": defaults.join_walk}
     start.update(start_point or {})
     t0 = time.time()
     best, best_t, trials = coordinate_descent(measure, start, sweeps=sweeps, log=log)

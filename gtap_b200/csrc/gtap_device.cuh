@@ -253,7 +253,8 @@ struct TaskHeader {
     uint8_t kind;     // task function index; kKindIndirect = use func table
     uint8_t flags;    // bits 0-2: spawn queue, bit 3: retain result for parent
     int32_t parent;   // parent tid, -1 for roots and orphans
-    int32_t join;     // bits 0-23: children still outstanding; bits 24-26: resume queue
+    int32_t join;     // bits 0-23: children still outstanding; bits 24-26: resume queue;
+                      // bit 27: the continuation only sums two int32 results (kJoinSumBit)
     int32_t root;     // root slot this task belongs to
 };
 static_assert(sizeof(TaskHeader) == kHdrBytes, "header must be 16 bytes");
@@ -262,6 +263,12 @@ constexpr uint8_t kFlagRetain = 0x8;
 constexpr uint8_t kFlagJoinFinish = 0x10;   // block mode: after its taskwait the task only finishes
 constexpr uint8_t kKindIndirect = 255;
 constexpr int kJoinCountMask = 0x00FFFFFF;
+// Thread mode: the task's code after its taskwait returns frame word 1 + frame
+// word 2 (int32, wrapping) into its parent's frame at the byte offset in frame
+// word 3 (into the root's result for a root task) and finishes.  The child
+// whose join decrement sees this bit with a count of one does exactly that in
+// place of resuming the task, and goes on to the grandparent's join.
+constexpr int kJoinSumBit = 1 << 27;
 
 // ---------------------------------------------------------------------------
 // MPMC ring of 32-bit values; each 64-bit slot = (lap + 1) << 32 | (value + 1)
@@ -295,6 +302,7 @@ struct Arena {
     int mode;               // GTAP_MODE_*
     int id_base;            // first id of the private ranges (ids below it are reserved)
     int publish_lazy;       // 0 or 1 for this launch (gtap_config::publish_lazy)
+    int join_walk;          // rounds of at most this many tasks run fib sums at their joins (gtap_config::join_walk)
     int max_inflight;       // admitted-but-unfinished roots allowed (0 = unlimited)
     int total_ids;          // ids in the arena
     unsigned long long watchdog_ns;

@@ -110,7 +110,10 @@ __device__ __forceinline__ void fib_task(const Arena& A, WarpShared& S, void* fr
             FibFrame* c2 = reinterpret_cast<FibFrame*>(
                 rt_spawn(A, S, K_FIB, epaq ? ((n - 2) < cutoff ? 1 : 0) : 0, &cc, nullptr, false, false));
             *reinterpret_cast<int4*>(c2) = make_int4(n - 2, 0, 0, 8);
-            if (rt_join(A, S, cc, 1, epaq ? 2 : 0)) return;
+            // the continuation below (return a + b) is the kJoinSumBit one: the
+            // child that completes the join may run it in place of resuming
+            // this task (gtap_config::join_walk)
+            if (rt_join(A, S, cc, 1, epaq ? 2 : 0, true)) return;
             fr = ld_data_v4(f);
         }
         // fallthrough
@@ -786,6 +789,7 @@ struct BuiltinProgramT {
     static constexpr int kFrameBytes = prog::kFrameBytes;
     static constexpr bool kFrameWords = true;    // exec gets the first 32 frame bytes
     static constexpr bool kFuncTable = false;    // kinds are dispatched by the switch below
+    static constexpr bool kJoinSum = true;       // fib's continuation runs at its join (kJoinSumBit)
     static constexpr int kLeafKeys = kSorts ? prog::kLeafKeys : 0;   // keys per leaf buffer (0: no warp leaves)
 
     __device__ static int root_kind(int k) {

@@ -364,7 +364,10 @@ __device__ __forceinline__ void* rt_spawn(const Arena& A, WarpShared& S, int kin
 }
 
 // taskwait: returns true if the task must suspend (children outstanding).
-__device__ __forceinline__ bool rt_join(const Arena& A, WarpShared& S, int child_count, int next_state, int q_after) {
+// then_sum: the task's code after this taskwait is the kJoinSumBit
+// continuation, which the child completing the join runs in place.
+__device__ __forceinline__ bool rt_join(const Arena& A, WarpShared& S, int child_count, int next_state, int q_after,
+                                        bool then_sum = false) {
     const unsigned lane = lane_id();
     if ((unsigned)q_after >= (unsigned)A.num_queues) {
         GTAP_ERROR(A, ERR_INVALID_QUEUE_IDX_AFTER_JOIN, S.l_tid[lane], q_after, q_after, A.num_queues);
@@ -380,7 +383,7 @@ __device__ __forceinline__ bool rt_join(const Arena& A, WarpShared& S, int child
     int4 hw;
     hw.x = (int)w0;
     hw.y = S.l_parent[lane];
-    hw.z = (child_count & kJoinCountMask) | (q_after << 24);
+    hw.z = (child_count & kJoinCountMask) | (q_after << 24) | (then_sum ? kJoinSumBit : 0);
     hw.w = S.l_root[lane];
     *reinterpret_cast<int4*>(hdr_of(A, S.l_tid[lane])) = hw;
     return true;
@@ -414,6 +417,38 @@ __device__ __forceinline__ void rt_release_id(const Arena& A, WarpShared& S, int
     } else {
         fence_acq_rel();
         ring_push_one(A.idpool, tid);
+    }
+}
+
+// One lane, after its join decrement brought task p's count to zero and
+// carried kJoinSumBit: p's continuation runs here instead of in a later round.
+// The acquiring decrement made the siblings' results in p's frame visible; the
+// sum goes into the grandparent's frame (or the root's result) and p finishes
+// (its id goes back, `finished` counts it for the root, which every task of the
+// chain shares).  The grandparent's join decrement releases the store; when it
+// completes that join too, the walk continues upwards.  Returns the task to
+// resume (a completed join without the bit, with its queue in rq), or -1.
+// Each step goes to a strict ancestor, so the walk ends within the tree's depth.
+static __device__ __noinline__ int join_sum_walk(const Arena& A, WarpShared& S, int p, int& finished, int& rq) {
+    for (;;) {
+        const int4 h = ld_cg_v4(hdr_of(A, p));
+        const int4 f = ld_cg_v4(frame_of(A, p));
+        const int gp = h.y;
+        const int v = (int)((unsigned)f.y + (unsigned)f.z);
+        if (gp >= 0) *reinterpret_cast<int*>(reinterpret_cast<char*>(frame_of(A, gp)) + f.w) = v;
+        else A.results[h.w].value = v;
+        rt_release_id_dbg(A, p);
+        if (!(((unsigned)h.x >> 24) & kFlagRetain)) rt_release_id(A, S, p);
+        ++finished;
+        if (gp < 0) return -1;
+        const int old = atom_add_acq_rel(&hdr_of(A, gp)->join, -1);
+        if ((old & kJoinCountMask) != 1) return -1;
+        if (!(old & kJoinSumBit)) {
+            rq = (old >> 24) & 7;
+            if (rq >= A.num_queues) rq = 0;
+            return gp;
+        }
+        p = gp;
     }
 }
 
@@ -1111,15 +1146,26 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
         GTAP_PHASE_ADD(12, ph2, ph3);
         // (3) joins: the last child re-enqueues its parent on the resume queue;
         //     release the finished task's id unless its parent reads its frame
-        int resumed = -1, rq = 0;
+        //     In a round of at most join_walk tasks, a completed join whose
+        //     continuation only sums two results runs that continuation here
+        //     (join_sum_walk), up the ancestors whose joins it completes;
+        //     `walked` counts the tasks it finished.  Fuller rounds resume
+        //     the parent as a task: a walk step costs dependent round trips
+        //     that a full round would wait for, while a resumed parent only
+        //     takes a lane of the next round.
+        int resumed = -1, rq = 0, walked = 0;
         if (my_fin) {
             const int parent = S.l_parent[lane];
             if (parent >= 0) {
                 const int old = atom_add_acq_rel(&hdr_of(A, parent)->join, -1);
                 if ((old & kJoinCountMask) == 1) {
-                    rq = (old >> 24) & 7;
-                    if (rq >= A.num_queues) rq = 0;
-                    resumed = parent;
+                    if (Prog::kJoinSum && (old & kJoinSumBit) && nb <= A.join_walk) {
+                        resumed = join_sum_walk(A, S, parent, walked, rq);
+                    } else {
+                        rq = (old >> 24) & 7;
+                        if (rq >= A.num_queues) rq = 0;
+                        resumed = parent;
+                    }
                 }
             }
             if (!(lane_flags & kLaneRetain)) {
@@ -1246,7 +1292,8 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
         if (one_root) {
             // every task of the round belongs to one root: warp sums, lane 0 books them
             const unsigned value = active ? (unsigned)S.l_value[lane] : 0u;
-            const int f_sum = __popc(fin);
+            const int w_sum = Prog::kJoinSum ? (int)__reduce_add_sync(0xffffffffu, (unsigned)walked) : 0;
+            const int f_sum = __popc(fin) + w_sum;
             const int v_sum = (int)__reduce_add_sync(0xffffffffu, value);
             if (lane == 0) {
                 if (v_sum) atomicAdd(reinterpret_cast<unsigned long long*>(&A.results[r0].value),
@@ -1261,6 +1308,7 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
             int f_sum = 0, v_sum = 0;
             if (active) {
                 f_sum = __popc(fin & grp);
+                if (Prog::kJoinSum) f_sum += (int)__reduce_add_sync(grp, (unsigned)walked);
                 v_sum = (int)__reduce_add_sync(grp, (unsigned)value);
             }
             const bool leader = active && ((unsigned)__ffs(grp) - 1u == lane);
@@ -1287,6 +1335,12 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
         }
         const unsigned created_all = __reduce_add_sync(0xffffffffu, (unsigned)(active ? S.l_created[lane] : 0));
         if (lane == 0) S.st[GTAP_STAT_TASKS] += created_all;
+#ifndef GTAP_PHASE_TIMERS
+        if (Prog::kJoinSum) {
+            const unsigned walked_all = __reduce_add_sync(0xffffffffu, (unsigned)walked);
+            if (lane == 0) S.st[GTAP_STAT_JOIN_FINISHES] += walked_all;
+        }
+#endif
         GTAP_PHASE_MARK(ph5);
         GTAP_PHASE_ADD(14, ph4, ph5);
         // (6) id cache

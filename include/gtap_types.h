@@ -93,6 +93,11 @@ typedef struct gtap_config {
     int32_t leaf_batch;      /* sort-capable kernel: sort and merge leaves a warp stages in shared memory
                                 at once, 1..8, 0 = 1 (one load round trip per batch; each costs 1 KB per
                                 warp of shared memory) */
+    int32_t join_walk;       /* thread mode, 0..32: in a round of at most this many tasks, the child that
+                                completes a built-in fib task's join runs the task's sum at once, and the
+                                ancestors' sums whose joins that completes, instead of resuming each in a
+                                later round (0 = never).  Each step costs dependent L2 round trips, so full
+                                rounds resume as usual; nearly empty rounds (the tree's drain) walk. */
 } gtap_config;
 
 /* Admission order of a batch (gtap_launch, gtap_run_host).  Results come back
@@ -155,7 +160,8 @@ enum {
     GTAP_STAT_PUBLISHED,          /* tasks made visible to thieves */
     GTAP_STAT_IDLE_POLLS,         /* idle-loop iterations */
     GTAP_STAT_OVERFLOW_PUSHES,
-    GTAP_STAT_JOIN_FINISHES,      /* block mode: continuations that only finish, booked at their join without running */
+    GTAP_STAT_JOIN_FINISHES,      /* continuations run at their join instead of as a task execution: block mode's
+                                     finish-only ones, thread mode's two-result sums (fib) */
     GTAP_STAT_IDLE_NS,            /* nanoseconds workers spent without a task (first failed acquire to the next
                                      success or exit); idle fraction = this / (workers x kernel time) */
     GTAP_STAT_COUNT = 16

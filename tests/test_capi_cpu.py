@@ -43,9 +43,9 @@ def test_struct_layouts_match_header():
     # sizes the C side uses (checked through offsets of the last fields)
     assert ctypes.sizeof(gt.Root) == 56
     assert ctypes.sizeof(gt.RootResult) == 40
-    assert ctypes.sizeof(gt.Config) == 88
     assert gt.Config.total_ids.offset == 40
     assert gt.Config.admit_order.offset == 80 and gt.Config.leaf_batch.offset == 84
+    assert gt.Config.join_walk.offset == 88 and ctypes.sizeof(gt.Config) == 96
     assert ctypes.sizeof(gt.RunStats) == 168
     assert gt.RunStats.light_kernel_ms.offset == 160
 
@@ -55,6 +55,7 @@ def test_default_config():
     assert c.mode == gt.MODE_THREAD and c.block % 32 == 0
     assert c.num_queues == 1 and c.steal_batch == 32
     assert c.deque_capacity & (c.deque_capacity - 1) == 0
+    assert c.join_walk == 0     # continuations resume as tasks unless a tuned configuration says otherwise
 
 
 def test_error_strings():

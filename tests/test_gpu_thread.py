@@ -43,7 +43,9 @@ def test_fib_cutoff0(rt, n):
     assert r.value == orc.fib(n)
     assert r.tasks == orc.fib_tasks(n, 0)
     assert st.counters[0] == orc.fib_tasks(n, 0)            # tasks created
-    assert st.counters[1] == orc.fib_executions(n, 0)       # executions incl. continuations
+    # every task body runs once, every continuation once: as an execution of
+    # its own, or at its join by the child that completes it (fib's sum)
+    assert st.counters[1] + st.counters[10] == orc.fib_executions(n, 0)
 
 
 def test_fib34_cutoff12(rt):
@@ -288,6 +290,42 @@ def test_overflow_queue_path():
 def test_epaq_fib_three_queues():
     # evaluation/3-epaq/fib/fib_queue_3.cu: leaves on queue 1, continuations on queue 2
     gt.gtap_initialize(gt.default_config(num_queues=4))
+    try:
+        r, st = run1(gt.fib_root(30, cutoff=13, epaq=True))
+        assert r.value == 832040 and r.tasks == orc.fib_tasks(30, 13)
+    finally:
+        gt.gtap_finalize()
+
+
+@pytest.mark.parametrize("join_walk", [1, 8, 32])
+def test_fib_sums_at_their_joins(join_walk):
+    """gtap_config.join_walk: in rounds of at most join_walk tasks, the child
+    that completes a fib task's join runs the task's sum and walks on to the
+    ancestors whose joins that completes.  Values and task counts stay the
+    oracle's; every continuation runs once, as an execution or at its join
+    (with 32 every round walks, so every sum runs at its join).  Batches mix
+    roots, so walks from different roots share rounds."""
+    gt.gtap_initialize(gt.default_config(join_walk=join_walk))
+    try:
+        for n, cutoff in ((2, 0), (20, 0), (30, 0), (34, 12)):
+            r, st = run1(gt.fib_root(n, cutoff))
+            assert r.status == gt.ROOT_DONE and r.value == orc.fib(n)
+            assert r.tasks == orc.fib_tasks(n, cutoff)
+            assert st.counters[1] + st.counters[10] == orc.fib_executions(n, cutoff)
+            if join_walk == 32:
+                assert st.counters[10] == orc.fib_executions(n, cutoff) - orc.fib_tasks(n, cutoff)
+        roots = [gt.fib_root(18 + i % 11) for i in range(64)] + [gt.nq_root(8 + i % 4) for i in range(64)]
+        res, st = gt.launch(roots)
+        for i, r in enumerate(res[:64]):
+            n = 18 + i % 11
+            assert r.status == gt.ROOT_DONE and r.value == orc.fib(n) and r.tasks == orc.fib_tasks(n, 0)
+        for i, r in enumerate(res[64:]):
+            n = 8 + i % 4
+            assert r.value == orc.nq(n) and r.tasks == orc.nq_tasks(n, n - 1)
+    finally:
+        gt.gtap_finalize()
+    # EPAQ: the walk ignores the continuation's queue, results do not change
+    gt.gtap_initialize(gt.default_config(num_queues=4, join_walk=join_walk))
     try:
         r, st = run1(gt.fib_root(30, cutoff=13, epaq=True))
         assert r.value == 832040 and r.tasks == orc.fib_tasks(30, 13)
