@@ -39,6 +39,7 @@ from gtap_b200.autotune import load_tuned  # noqa: E402
 METRIC = "tasks_per_sec_batched_4096_root_mix"
 UNIT = "tasks/s"
 TUNED = os.path.join(ROOT, "gtap_b200", "tuned", "b200_mix.json")
+BLOCK_TUNED = os.path.join(ROOT, "gtap_b200", "tuned", "b200_cilksort26_block.json")
 
 # algorithmic bytes per task (frame S written by the parent + read by the child,
 # 8 B deque slot, 8 B join RMW, 4 B result), frame sizes of the lowered tasks
@@ -431,7 +432,8 @@ def main():
         gt.gtap_finalize()
         block = measure_block_cilksort(gt, args.block_keys, args.steps, args.warmup,
                                        cpu=not args.no_cpu and rank == 0 and world == 1, hbm_peak=hbm,
-                                       overrides=json.loads(args.config) if args.config else {})
+                                       overrides=json.loads(args.config) if args.config else {},
+                                       tuned=BLOCK_TUNED if args.tuned else "")
 
     # thread mode: mergesort of mt19937(42) keys (examples/mergesort/mergesort.cu's cutoff 128)
     msort = None
@@ -552,17 +554,21 @@ def measure_mergesort_thread(gt, n, steps, warmup, hbm_peak, overrides=None):
                          "kernel": "gtap::thread_worker_kernel<BuiltinProgram>"}}
 
 
-def measure_block_cilksort(gt, n, steps, warmup, cpu, hbm_peak, overrides=None):
+def measure_block_cilksort(gt, n, steps, warmup, cpu, hbm_peak, overrides=None, tuned=""):
     """cilksort of n keys (std::mt19937(42), full int32 range) in block mode,
     one root per launch, inputs resident; leaves read the pristine input so
-    no restore is needed between launches.  Checked against a plain sort."""
+    no restore is needed between launches.  Checked against a plain sort.
+    The configuration: the block-mode tuner result `tuned` (library defaults
+    without one), then the explicit overrides."""
     import torch
     keys = gt.gen_keys(42, n)
     src = torch.from_numpy(keys).cuda()
     arr = torch.empty_like(src)
     tmp = torch.empty_like(src)
-    # library defaults (the tuned file is for thread mode) plus explicit overrides
-    gt.gtap_initialize(gt.default_config(**dict(overrides or {}, mode=gt.MODE_BLOCK)))
+    over = load_tuned(tuned) if tuned else {}
+    over.update(overrides or {})
+    over["mode"] = gt.MODE_BLOCK
+    gt.gtap_initialize(gt.default_config(**over))
     root = gt.cilksort_root(src.data_ptr(), arr.data_ptr(), tmp.data_ptr(), n, 2048, 2048)
     for _ in range(max(1, warmup)):
         res, st = gt.launch([root])
@@ -580,6 +586,7 @@ def measure_block_cilksort(gt, n, steps, warmup, cpu, hbm_peak, overrides=None):
                        "cutoffs 2048, one root per launch" % n,
            "keys": n, "ms_per_sort": k_ms, "keys_per_s": n / (k_ms / 1e3), "tasks": tasks,
            "tasks_per_s": tasks / (k_ms / 1e3), "grid": st.grid, "block": st.block,
+           "config": os.path.relpath(tuned, ROOT) if tuned and load_tuned(tuned) else "library defaults",
            "executions": int(st.counters[1]), "join_finishes": int(st.counters[10]),
            "steal_success_rate": int(st.counters[4]) / max(1, int(st.counters[3])),
            "sorted_equals_plain_sort": ok,

@@ -36,6 +36,7 @@ configuration that breaks a result cannot win.
 
     python -m gtap_b200.autotune --workload mix --out gtap_b200/tuned/b200_mix.json
     python -m gtap_b200.autotune --workload serve --out gtap_b200/tuned/b200_serve.json
+    python -m gtap_b200.autotune --workload cilksort26_block --out gtap_b200/tuned/b200_cilksort26_block.json
 
 The serve workload is the served roots (BFS on R-MAT 16-20, tree sums of
 2^18-2^20 nodes, 200 of them) in one batch launch of the kernel serve mode
@@ -133,7 +134,9 @@ def run(workload="mix", reps=3, sweeps=2, n_roots=None, out=None, quiet=False, s
     sm_count = torch.cuda.get_device_properties(0).multi_processor_count
     keep = []
     before = None   # runs before every launch (resets what a launch consumes)
+    check = None    # checks the warm-up launch's output beyond values and task counts
     fixed = {}      # overrides every trial carries
+    space, order = SPACE, ORDER
     if workload == "mix":
         mix = wl.Mix(gt, n_roots or wl.N_ROOTS)
         src, arr, tmp = mix.device_slabs()
@@ -153,6 +156,23 @@ def run(workload="mix", reps=3, sweeps=2, n_roots=None, out=None, quiet=False, s
             for d in depths:
                 if d is not None:
                     d.fill_(0x3f3f3f3f)
+    elif workload == "cilksort26_block":
+        # block-cooperative cilksort of 2^26 mt19937(42) keys, cutoffs
+        # 2048/2048; one worker per block, so warps per SM reach 64 and only
+        # the axes the block scheduler reads are searched
+        n = n_roots or (1 << 26)
+        src = torch.from_numpy(gt.gen_keys(42, n)).cuda()
+        arr = torch.empty_like(src)
+        tmp = torch.empty_like(src)
+        want = torch.sort(src).values
+        keep += [src, arr, tmp, want]
+        roots = [gt.cilksort_root(src.data_ptr(), arr.data_ptr(), tmp.data_ptr(), n, 2048, 2048)]
+        fixed["mode"] = gt.MODE_BLOCK
+        space = dict(SPACE, warps_per_sm=[16, 32, 48, 64], block=[64, 128, 256, 512])
+        order = ["warps_per_sm", "block", "deque_capacity", "probe_width", "victim_policy"]
+
+        def check():
+            return bool(torch.equal(arr, want))
     else:
         roots = wl.single_root_workload(gt, workload)
     kinds = [r.kind for r in roots]
@@ -171,6 +191,8 @@ def run(workload="mix", reps=3, sweeps=2, n_roots=None, out=None, quiet=False, s
             if before:
                 before()
             res, st = gt.launch(roots)                      # warm-up
+            if check is not None and not check():
+                raise RuntimeError("configuration %s gave a wrong output" % over)
             sig = _signature(gt, res, kinds)
             if "sig" not in ref_sig:
                 ref_sig["sig"] = sig
@@ -199,9 +221,12 @@ def run(workload="mix", reps=3, sweeps=2, n_roots=None, out=None, quiet=False, s
              "spawn_capacity": defaults.spawn_capacity, "max_inflight_roots": defaults.max_inflight_roots,
              "publish_lazy": defaults.publish_lazy, "leaf_batch": defaults.leaf_batch,
              "join_walk": defaults.join_walk}
+    if workload == "cilksort26_block":
+        start = {"warps_per_sm": 64, "block": defaults.block, "deque_capacity": defaults.deque_capacity,
+                 "probe_width": defaults.probe_width, "victim_policy": defaults.victim_policy}
     start.update(start_point or {})
     t0 = time.time()
-    best, best_t, trials = coordinate_descent(measure, start, sweeps=sweeps, log=log)
+    best, best_t, trials = coordinate_descent(measure, start, space=space, order=order, sweeps=sweeps, log=log)
     best_over = to_overrides(best, sm_count)
     best_over.update(fixed)
     result = {"workload": workload, "roots": len(roots), "device": torch.cuda.get_device_name(0),
@@ -228,7 +253,8 @@ def load_tuned(path):
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    ap.add_argument("--workload", default="mix", choices=["mix", "serve", "fib30", "fib34c12", "nq13", "nq13c7"])
+    ap.add_argument("--workload", default="mix",
+                    choices=["mix", "serve", "fib30", "fib34c12", "nq13", "nq13c7", "cilksort26_block"])
     ap.add_argument("--roots", type=int, default=None)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--sweeps", type=int, default=2)

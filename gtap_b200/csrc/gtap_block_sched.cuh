@@ -48,6 +48,8 @@ struct BlockShared {
     int finished;
     long long value;                 // contributions to the root's value
     int next;                        // task to run next (continuation first), -1 none
+    unsigned long long dq_word;      // this block's deque control word as last seen: tag and bottom exact
+                                     // (only the owner moves them), top possibly behind (thieves move it)
     int pre_task;                    // the task whose record round end already loaded into the fields above
     int stop;
     int worker;
@@ -291,19 +293,28 @@ __device__ __forceinline__ void bt_prof_working(const Arena& A, BlockShared& S) 
 // ---------------------------------------------------------------------------
 // scheduling (warp 0; lane 0 unless noted)
 // ---------------------------------------------------------------------------
-// Owner pop, newest first (reference pop :327-361, as one CAS on the control word).
+// Owner pop, newest first (reference pop :327-361, as one CAS on the control
+// word).  The CAS starts from the cached word: its size can only overstate the
+// deque's (thieves only advance top), so an empty cache means an empty deque,
+// and a stale top fails the CAS, which returns the current word.  The slot
+// load goes out with the CAS: this block wrote that slot, and the value is
+// used only if the CAS claims it.  One round trip when no thief interferes.
 static __device__ int bt_pop_own(const Arena& A, BlockShared& S) {
     unsigned long long* c = dq_ctl_ptr(A, 0, S.worker);
-    unsigned long long wv = ld_relaxed(c);
+    unsigned long long wv = S.dq_word;
     for (int i = 0; i < 16; ++i) {
-        if (dq_size(wv) == 0) return -1;
-        const unsigned long long old = atom_cas_acquire(c, wv, dq_owner_pop(wv, 1));
+        if (dq_size(wv) == 0) break;
+        const int id = ld_relaxed(dq_slot_ptr(A, 0, S.worker, dq_bottom(wv) - 1u));
+        const unsigned long long nw = dq_owner_pop(wv, 1);
+        const unsigned long long old = atom_cas_acquire(c, wv, nw);
         if (old == wv) {
+            S.dq_word = nw;
             S.st[GTAP_STAT_POPS] += 1;
-            return ld_relaxed(dq_slot_ptr(A, 0, S.worker, dq_bottom(wv) - 1u));
+            return id;
         }
         wv = old;
     }
+    S.dq_word = wv;
     return -1;
 }
 
@@ -500,9 +511,9 @@ static __device__ void bt_round_end(const Arena& A, BlockShared& S) {
     int direct = 0;
     unsigned long long* c = dq_ctl_ptr(A, 0, S.worker);
     if (m > 0) {
-        unsigned long long wv = 0;
-        if (lane == 0) wv = ld_relaxed(c);
-        wv = __shfl_sync(0xffffffffu, wv, 0);
+        // the cached control word: bottom exact, the size at most overstated
+        // (a thief's steal may not be in it), so the room is never overstated
+        const unsigned long long wv = S.dq_word;
         const unsigned cap = 1u << A.deque_cap_log2;
         const unsigned used = dq_size(wv);
         b = dq_bottom(wv);
@@ -511,7 +522,10 @@ static __device__ void bt_round_end(const Arena& A, BlockShared& S) {
     }
     __syncwarp();
     // one fence orders the body's stores (the whole block's, through the
-    // barrier before this), the records and the slots before what follows
+    // barrier before this), the records and the slots before what follows.
+    // (For a finished task that publishes nothing, an acquire-release join
+    // decrement in place of this fence and an acquire-only one measured
+    // slower: 12.40 against 12.23 ms for 2^26 keys.)
     if (lane == 0) fence_acq_rel();
     __syncwarp();
     if (m > direct) {
@@ -525,6 +539,7 @@ static __device__ void bt_round_end(const Arena& A, BlockShared& S) {
     if (lane == 0) {
         if (direct > 0) {
             red_add_relaxed(c, (unsigned long long)direct << kPosBits);
+            S.dq_word += (unsigned long long)direct << kPosBits;
             S.st[GTAP_STAT_PUBLISHED] += (unsigned long long)direct;
         }
         int next = kept;
@@ -629,6 +644,7 @@ __device__ void block_worker(const Arena& A, BlockShared& S, int* smem, int init
     if (tid == 0) {
         S.worker = blockIdx.x;
         S.next = initial_tid;
+        S.dq_word = ld_relaxed(dq_ctl_ptr(A, 0, blockIdx.x));   // reset before the launch
         S.pre_task = -1;
         S.stop = 0;
         S.task = -1;
