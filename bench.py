@@ -40,6 +40,7 @@ METRIC = "tasks_per_sec_batched_4096_root_mix"
 UNIT = "tasks/s"
 TUNED = os.path.join(ROOT, "gtap_b200", "tuned", "b200_mix.json")
 BLOCK_TUNED = os.path.join(ROOT, "gtap_b200", "tuned", "b200_cilksort26_block.json")
+MSORT_TUNED = os.path.join(ROOT, "gtap_b200", "tuned", "b200_mergesort24.json")
 
 # algorithmic bytes per task (frame S written by the parent + read by the child,
 # 8 B deque slot, 8 B join RMW, 4 B result), frame sizes of the lowered tasks
@@ -440,7 +441,8 @@ def main():
     if args.mergesort_keys > 0:
         gt.gtap_finalize()
         msort = measure_mergesort_thread(gt, args.mergesort_keys, args.steps, args.warmup, hbm_peak=hbm,
-                                         overrides=json.loads(args.config) if args.config else {})
+                                         overrides=json.loads(args.config) if args.config else {},
+                                         tuned=MSORT_TUNED if args.tuned else "")
 
     # the reference GTaP GPU build on fib, beside this runtime (same box, same call),
     # and as the per-root baseline for the mix's fib roots
@@ -523,16 +525,19 @@ def mergesort_bytes(n, cutoff):
     return 8 * n + mergesort_bytes(nl, cutoff) + mergesort_bytes(n - nl, cutoff)
 
 
-def measure_mergesort_thread(gt, n, steps, warmup, hbm_peak, overrides=None):
+def measure_mergesort_thread(gt, n, steps, warmup, hbm_peak, overrides=None, tuned=""):
     """mergesort of n keys (std::mt19937(42)) in thread mode, cutoff 128 and
-    merge cutoff 256, one root per launch with the library defaults (plus
-    explicit overrides); checked against a plain sort."""
+    merge cutoff 256, one root per launch with the tuner's result `tuned`
+    (library defaults without one) plus explicit overrides; checked against a
+    plain sort."""
     import torch
     keys = gt.gen_keys(42, n)
     src = torch.from_numpy(keys).cuda()
     out = torch.empty_like(src)
     tmp = torch.empty_like(src)
-    gt.gtap_initialize(gt.default_config(**dict(overrides or {})))
+    over = load_tuned(tuned) if tuned else {}
+    over.update(overrides or {})
+    gt.gtap_initialize(gt.default_config(**over))
     root = gt.mergesort_root(src.data_ptr(), out.data_ptr(), tmp.data_ptr(), n, 128, 256)
     for _ in range(max(1, warmup)):
         res, st = gt.launch([root])
@@ -549,6 +554,7 @@ def measure_mergesort_thread(gt, n, steps, warmup, hbm_peak, overrides=None):
                         "one root per launch" % n,
             "keys": n, "ms_per_sort": k_ms, "keys_per_s": n / (k_ms / 1e3), "tasks": res[0].tasks,
             "tasks_per_s": res[0].tasks / (k_ms / 1e3), "sorted_equals_plain_sort": ok,
+            "config": os.path.relpath(tuned, ROOT) if tuned and load_tuned(tuned) else "library defaults",
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak, "algorithmic_bytes_per_launch": alg,
                          "kernel": "gtap::thread_worker_kernel<BuiltinProgram>"}}

@@ -37,6 +37,7 @@ configuration that breaks a result cannot win.
     python -m gtap_b200.autotune --workload mix --out gtap_b200/tuned/b200_mix.json
     python -m gtap_b200.autotune --workload serve --out gtap_b200/tuned/b200_serve.json
     python -m gtap_b200.autotune --workload cilksort26_block --out gtap_b200/tuned/b200_cilksort26_block.json
+    python -m gtap_b200.autotune --workload mergesort24 --out gtap_b200/tuned/b200_mergesort24.json
 
 The serve workload is the served roots (BFS on R-MAT 16-20, tree sums of
 2^18-2^20 nodes, 200 of them) in one batch launch of the kernel serve mode
@@ -173,6 +174,21 @@ def run(workload="mix", reps=3, sweeps=2, n_roots=None, out=None, quiet=False, s
 
         def check():
             return bool(torch.equal(arr, want))
+    elif workload == "mergesort24":
+        # thread-mode mergesort of 2^24 mt19937(42) keys, cutoff 128 and merge
+        # cutoff 256 (examples/mergesort/mergesort.cu's settings)
+        n = n_roots or (1 << 24)
+        src = torch.from_numpy(gt.gen_keys(42, n)).cuda()
+        arr = torch.empty_like(src)
+        tmp = torch.empty_like(src)
+        want = torch.sort(src).values
+        keep += [src, arr, tmp, want]
+        roots = [gt.mergesort_root(src.data_ptr(), arr.data_ptr(), tmp.data_ptr(), n, 128, 256)]
+        order = ["warps_per_sm", "block", "leaf_batch", "spawn_capacity", "steal_batch", "deque_capacity",
+                 "probe_width", "victim_policy", "publish_lazy"]
+
+        def check():
+            return bool(torch.equal(arr, want))
     else:
         roots = wl.single_root_workload(gt, workload)
     kinds = [r.kind for r in roots]
@@ -254,7 +270,7 @@ def load_tuned(path):
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--workload", default="mix",
-                    choices=["mix", "serve", "fib30", "fib34c12", "nq13", "nq13c7", "cilksort26_block"])
+                    choices=["mix", "serve", "fib30", "fib34c12", "nq13", "nq13c7", "cilksort26_block", "mergesort24"])
     ap.add_argument("--roots", type=int, default=None)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--sweeps", type=int, default=2)
