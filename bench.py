@@ -550,6 +550,7 @@ def measure_mergesort_thread(gt, n, steps, warmup, hbm_peak, overrides=None, tun
     k_ms = statistics.mean(ms)
     alg = mergesort_bytes(n, 128)
     achieved = alg / (k_ms / 1e3) / 1e9
+    ratio = traffic_from_profile("mergesort_kernel_traffic_over_algorithmic")
     return {"workload": "mergesort of %d int32 keys (std::mt19937(42)), thread mode, cutoff 128, merge cutoff 256, "
                         "one root per launch" % n,
             "keys": n, "ms_per_sort": k_ms, "keys_per_s": n / (k_ms / 1e3), "tasks": res[0].tasks,
@@ -557,6 +558,7 @@ def measure_mergesort_thread(gt, n, steps, warmup, hbm_peak, overrides=None, tun
             "config": os.path.relpath(tuned, ROOT) if tuned and load_tuned(tuned) else "library defaults",
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak, "algorithmic_bytes_per_launch": alg,
+                         "traffic": None if ratio is None else int(alg * ratio),
                          "kernel": "gtap::thread_worker_kernel<BuiltinProgram>"}}
 
 
