@@ -55,7 +55,7 @@ class Config(ctypes.Structure):
         ("admit_batch", ctypes.c_int32), ("watchdog_ms", ctypes.c_int64), ("profile_samples", ctypes.c_int32),
         ("result_handles", ctypes.c_int32), ("publish_lazy", ctypes.c_int32), ("max_inflight_roots", ctypes.c_int32),
         ("admit_order", ctypes.c_int32), ("leaf_batch", ctypes.c_int32),
-        ("join_walk", ctypes.c_int32),
+        ("join_walk", ctypes.c_int32), ("sub_rounds", ctypes.c_int32),
     ]
 
     def as_dict(self):

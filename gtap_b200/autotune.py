@@ -24,6 +24,8 @@ Search: coordinate descent from the library defaults over
                  2: 1 without sort leaves, 0 in the sorting kernel
   join_walk      rounds of at most this many tasks run fib's sums at their joins
                  (0: never); the tree's drain gains, full rounds would wait
+  sub_rounds     extra passes of task bodies on a round's idle lanes over the
+                 children the round staged (fib / n-queens launches)
   max_inflight_roots  roots admitted and not finished, at most (0: no limit);
                  an asynchronous BFS relaxes vertices more than once the more
                  roots share the GPU, so served batches of BFS roots do less
@@ -66,9 +68,10 @@ SPACE = {
     "publish_lazy": [0, 1, 2],
     "leaf_batch": [1, 2, 4],
     "join_walk": [0, 2, 4, 8, 32],
+    "sub_rounds": [0, 1, 2, 4, 8],
 }
 ORDER = ["publish_lazy", "max_inflight_roots", "leaf_batch", "warps_per_sm", "block", "steal_batch", "deque_capacity", "probe_width",
-         "victim_policy", "num_queues", "spawn_capacity", "join_walk"]
+         "victim_policy", "num_queues", "spawn_capacity", "join_walk", "sub_rounds"]
 
 
 def to_overrides(point, sm_count):
@@ -236,7 +239,7 @@ def run(workload="mix", reps=3, sweeps=2, n_roots=None, out=None, quiet=False, s
              "victim_policy": defaults.victim_policy, "num_queues": defaults.num_queues,
              "spawn_capacity": defaults.spawn_capacity, "max_inflight_roots": defaults.max_inflight_roots,
              "publish_lazy": defaults.publish_lazy, "leaf_batch": defaults.leaf_batch,
-             "join_walk": defaults.join_walk}
+             "join_walk": defaults.join_walk, "sub_rounds": defaults.sub_rounds}
     if workload == "cilksort26_block":
         start = {"warps_per_sm": 64, "block": defaults.block, "deque_capacity": defaults.deque_capacity,
                  "probe_width": defaults.probe_width, "victim_policy": defaults.victim_policy}

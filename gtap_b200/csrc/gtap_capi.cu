@@ -163,7 +163,8 @@ bool roots_need_sorts(const gtap_root* roots, int n) {
 
 // layouts the Python binding and other FFI callers mirror
 static_assert(sizeof(gtap_config) == 96 && offsetof(gtap_config, admit_order) == 80 &&
-                  offsetof(gtap_config, leaf_batch) == 84 && offsetof(gtap_config, join_walk) == 88,
+                  offsetof(gtap_config, leaf_batch) == 84 && offsetof(gtap_config, join_walk) == 88 &&
+                  offsetof(gtap_config, sub_rounds) == 92,
               "gtap_config layout");
 static_assert(sizeof(gtap_run_stats) == 168 && offsetof(gtap_run_stats, light_kernel_ms) == 160,
               "gtap_run_stats layout");
@@ -310,6 +311,7 @@ Arena make_arena(int n_roots, int mode, int workers, int first_root = 0) {
     A.mode = mode;
     A.publish_lazy = c.publish_lazy != 0 ? 1 : 0;
     A.join_walk = c.join_walk;
+    A.sub_rounds = c.sub_rounds;
     A.max_inflight = c.max_inflight_roots;
     A.total_ids = (int)c.total_ids;
     A.watchdog_ns = (unsigned long long)c.watchdog_ms * 1000000ull;
@@ -401,6 +403,7 @@ int validate_config(const gtap_config& c) {
     if (c.admit_order < GTAP_ADMIT_AS_GIVEN || c.admit_order > GTAP_ADMIT_SPLIT) return GTAP_ERROR_INVALID_ARGUMENT;
     if (c.leaf_batch < 0 || c.leaf_batch > 8) return GTAP_ERROR_INVALID_ARGUMENT;
     if (c.join_walk < 0 || c.join_walk > 32) return GTAP_ERROR_INVALID_ARGUMENT;
+    if (c.sub_rounds < 0 || c.sub_rounds > 8) return GTAP_ERROR_INVALID_ARGUMENT;
     return 0;
 }
 
@@ -699,6 +702,7 @@ int gtap_default_config(gtap_config* cfg) {
     cfg->admit_order = GTAP_ADMIT_SPLIT;
     cfg->leaf_batch = 1;
     cfg->join_walk = 0;
+    cfg->sub_rounds = 0;
     return 0;
 }
 

@@ -303,6 +303,7 @@ struct Arena {
     int id_base;            // first id of the private ranges (ids below it are reserved)
     int publish_lazy;       // 0 or 1 for this launch (gtap_config::publish_lazy)
     int join_walk;          // rounds of at most this many tasks run fib sums at their joins (gtap_config::join_walk)
+    int sub_rounds;         // extra passes of task bodies on a round's idle lanes (gtap_config::sub_rounds)
     int max_inflight;       // admitted-but-unfinished roots allowed (0 = unlimited)
     int total_ids;          // ids in the arena
     unsigned long long watchdog_ns;

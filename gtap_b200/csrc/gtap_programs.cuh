@@ -790,6 +790,9 @@ struct BuiltinProgramT {
     static constexpr bool kFrameWords = true;    // exec gets the first 32 frame bytes
     static constexpr bool kFuncTable = false;    // kinds are dispatched by the switch below
     static constexpr bool kJoinSum = true;       // fib's continuation runs at its join (kJoinSumBit)
+    // extra passes on idle lanes (gtap_config::sub_rounds): only in the fib /
+    // n-queens kernel, whose registers have room for the pass loop
+    static constexpr bool kSubRounds = !kSorts && !kGraphs;
     static constexpr int kLeafKeys = kSorts ? prog::kLeafKeys : 0;   // keys per leaf buffer (0: no warp leaves)
 
     __device__ static int root_kind(int k) {

@@ -1010,7 +1010,17 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
         unsigned long long fn = 0;
         int bad = 0;
         if (staged) rec_stage_wait();
-        if ((int)lane < nb) {
+        // Lanes [run_lo, nb) run a task in this pass.  With sub_rounds > 0, a
+        // round whose tasks leave lanes idle runs up to sub_rounds more passes
+        // on them, each over the newest children the passes before it staged
+        // (they would otherwise wait for the next round): a tree's ramp-up
+        // and drain go down several levels per round.
+        int run_lo = 0;
+#ifdef GTAP_PHASE_TIMERS
+        long long ph1b = 0;
+#endif
+        for (int pass = 0;; ++pass) {
+        if ((int)lane >= run_lo && (int)lane < nb) {
             if ((unsigned)my_tid >= (unsigned)A.total_ids) {
                 bad = 1;
             } else {
@@ -1018,7 +1028,7 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
                 // through a function table) the task function, in one round
                 // trip, or from the record stage the previous round filled
                 const char* rec = A.records + (size_t)my_tid * A.rec_stride;
-                if (staged) {
+                if (staged && pass == 0) {
                     const int4* st4 = S.rstage + lane * 3;
                     hw = st4[0];
                     if (Prog::kFrameWords) {
@@ -1037,17 +1047,22 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
             }
             if (bad) GTAP_ERROR(A, ERR_INVALID_ARGUMENT, my_tid, -1, bad == 1 ? my_tid : hw.w, A.total_ids);
         }
-        if (__any_sync(0xffffffffu, bad)) break;   // corrupted id or header: stop this worker, launch aborts
-        GTAP_PHASE_MARK_AFTER(ph1b, hw.x ^ fw0.x ^ fw1.w ^ (int)fn);
-        GTAP_PHASE_ADD(9, ph1, ph1b);
+        if (__any_sync(0xffffffffu, bad)) break;   // corrupted id or header: leaves the passes, then the loop
+#ifdef GTAP_PHASE_TIMERS
+        if (pass == 0) {
+            GTAP_PHASE_MARK_AFTER(ph1b_, hw.x ^ fw0.x ^ fw1.w ^ (int)fn);
+            GTAP_PHASE_ADD(9, ph1, ph1b_);
+            ph1b = ph1b_;
+        }
+#endif
 #ifdef GTAP_DEBUG_IDS
-        if ((int)lane < nb) {
+        if ((int)lane >= run_lo && (int)lane < nb) {
             if (ld_cg(&A.dbg_live[my_tid]) != 1) GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, my_tid, src_kind, 3, (int)lane * 1000 + nb);
             int prev = atomicAdd(&A.dbg_exec[my_tid], 1);
             if ((hw.x & 0xFFFF) == 0 && prev != 0) GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, my_tid, -1, 5, prev);
         }
 #endif
-        if ((int)lane < nb) {
+        if ((int)lane >= run_lo && (int)lane < nb) {
             S.l_tid[lane] = my_tid;
             S.l_w0[lane] = (unsigned)hw.x;
             S.l_parent[lane] = hw.y;
@@ -1057,6 +1072,28 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
             Prog::exec(A, S, (int)(((unsigned)hw.x >> 16) & 0xFFu), my_tid, frame_of(A, my_tid), fw0, fw1, fn);
         }
         __syncwarp();
+        // another pass: single queue, every staged child in the buffer, and
+        // no task of the round returned with children outstanding (those
+        // children become orphans at round end, so none may run before it)
+        if (!Prog::kSubRounds || pass >= A.sub_rounds || nb >= kWarp) break;
+        {
+            const int have = S.cnt[0];
+            const bool orphans = __any_sync(0xffffffffu, (int)lane < nb && (S.l_flags[lane] & kLaneFinished) &&
+                                                             S.l_spawned[lane] > 0);
+            if (A.num_queues != 1 || have <= 0 || have > A.spawn_cap || orphans) break;
+            const int k = min(have, kWarp - nb);
+            // lane nb + j takes the j-th newest staged child; the staging
+            // entries were written (and the children's records and frames)
+            // before the warp barrier above
+            if ((int)lane >= nb && (int)lane < nb + k) my_tid = S.sbuf[have - 1 - ((int)lane - nb)] & kIdMask;
+            __syncwarp();
+            if (lane == 0) S.cnt[0] = have - k;
+            __syncwarp();
+            run_lo = nb;
+            nb += k;
+        }
+        }
+        if (__any_sync(0xffffffffu, bad)) break;   // corrupted id or header: stop this worker, launch aborts
         GTAP_PHASE_MARK(ph2);
         GTAP_PHASE_ADD(11, ph1b, ph2);
         // ---- leaf work the round's tasks left for the whole warp ----

@@ -161,6 +161,7 @@ struct Program {
 #endif
     static constexpr bool kFuncTable = true;
     static constexpr bool kJoinSum = false;   // every continuation runs as a task
+    static constexpr bool kSubRounds = false; // one pass of task bodies per round
     __device__ static int root_kind(int) { return -1; }   // roots come from __gtap_push_initial_task only
     __device__ static bool root_args_ok(const gtap_root&) { return true; }
     __device__ static void init_root(const gtap::Arena&, const gtap_root&, void*) {}

@@ -98,6 +98,12 @@ typedef struct gtap_config {
                                 ancestors' sums whose joins that completes, instead of resuming each in a
                                 later round (0 = never).  Each step costs dependent L2 round trips, so full
                                 rounds resume as usual; nearly empty rounds (the tree's drain) walk. */
+    int32_t sub_rounds;      /* thread mode, 0..8, single queue, launches of fib and n-queens roots only (the
+                                kernel without BFS, tree-sum and sort bodies): a round that leaves lanes idle runs up to this
+                                many more passes of task bodies on them, each over the newest children the
+                                passes before it staged, instead of leaving those children to the next round
+                                (0 = one pass).  A tree's ramp-up and drain then go down several levels per
+                                round. */
 } gtap_config;
 
 /* Admission order of a batch (gtap_launch, gtap_run_host).  Results come back

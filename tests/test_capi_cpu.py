@@ -45,7 +45,8 @@ def test_struct_layouts_match_header():
     assert ctypes.sizeof(gt.RootResult) == 40
     assert gt.Config.total_ids.offset == 40
     assert gt.Config.admit_order.offset == 80 and gt.Config.leaf_batch.offset == 84
-    assert gt.Config.join_walk.offset == 88 and ctypes.sizeof(gt.Config) == 96
+    assert gt.Config.join_walk.offset == 88 and gt.Config.sub_rounds.offset == 92
+    assert ctypes.sizeof(gt.Config) == 96
     assert ctypes.sizeof(gt.RunStats) == 168
     assert gt.RunStats.light_kernel_ms.offset == 160
 
@@ -56,6 +57,7 @@ def test_default_config():
     assert c.num_queues == 1 and c.steal_batch == 32
     assert c.deque_capacity & (c.deque_capacity - 1) == 0
     assert c.join_walk == 0     # continuations resume as tasks unless a tuned configuration says otherwise
+    assert c.sub_rounds == 0    # one pass of task bodies per round
 
 
 def test_error_strings():

@@ -331,3 +331,35 @@ def test_fib_sums_at_their_joins(join_walk):
         assert r.value == 832040 and r.tasks == orc.fib_tasks(30, 13)
     finally:
         gt.gtap_finalize()
+
+
+@pytest.mark.parametrize("sub_rounds", [1, 8])
+def test_sub_rounds_on_idle_lanes(sub_rounds):
+    """gtap_config.sub_rounds: a round with idle lanes runs more passes of task
+    bodies on them over the children staged in the round.  Values, task
+    counts and executions stay the oracle's, alone and with the join walk,
+    for single roots (whose ramp-up and drain leave lanes idle) and for a
+    batch of fib and n-queens roots."""
+    for join_walk in (0, 32):
+        gt.gtap_initialize(gt.default_config(sub_rounds=sub_rounds, join_walk=join_walk))
+        try:
+            for n, cutoff in ((1, 0), (2, 0), (20, 0), (30, 0), (34, 12)):
+                r, st = run1(gt.fib_root(n, cutoff))
+                assert r.status == gt.ROOT_DONE and r.value == orc.fib(n)
+                assert r.tasks == orc.fib_tasks(n, cutoff)
+                assert st.counters[1] + st.counters[10] == orc.fib_executions(n, cutoff)
+            for n in (1, 8, 12, 13):
+                r, st = run1(gt.nq_root(n))
+                assert r.value == orc.nq(n) and r.tasks == orc.nq_tasks(n, n - 1)
+            r, st = run1(gt.nq_root(13, 7))
+            assert r.value == orc.nq(13) and r.tasks == orc.nq_tasks(13, 7)
+            roots = [gt.fib_root(18 + i % 11) for i in range(48)] + [gt.nq_root(8 + i % 4) for i in range(48)]
+            res, st = gt.launch(roots)
+            for i, r in enumerate(res[:48]):
+                n = 18 + i % 11
+                assert r.status == gt.ROOT_DONE and r.value == orc.fib(n) and r.tasks == orc.fib_tasks(n, 0)
+            for i, r in enumerate(res[48:]):
+                n = 8 + i % 4
+                assert r.value == orc.nq(n) and r.tasks == orc.nq_tasks(n, n - 1)
+        finally:
+            gt.gtap_finalize()
