@@ -85,6 +85,10 @@ static __device__ __noinline__ int fib_sequential(int n) {
     return (int)sum;
 }
 
+// kPair: both children through rt_spawn_pair (one id-cache and one staging
+// claim for the two); used in the fib / n-queens kernel, whose registers have
+// room for it (the other kernels spill with it).
+template <bool kPair>
 __device__ __forceinline__ void fib_task(const Arena& A, WarpShared& S, void* frame, const int4& w0) {
     FibFrame* f = reinterpret_cast<FibFrame*>(frame);
     int4 fr = w0;   // {n, a, b, slot}, loaded with the header
@@ -104,11 +108,15 @@ __device__ __forceinline__ void fib_task(const Arena& A, WarpShared& S, void* fr
             }
             const bool epaq = rd.i2 != 0 && A.num_queues >= 3;
             int cc = 0;
-            FibFrame* c1 = reinterpret_cast<FibFrame*>(
-                rt_spawn(A, S, K_FIB, epaq ? ((n - 1) < cutoff ? 1 : 0) : 0, &cc, nullptr, false, false));
+            void* c1;
+            void* c2;
+            if (kPair && !epaq) {
+                rt_spawn_pair(A, S, K_FIB, &cc, &c1, &c2);
+            } else {
+                c1 = rt_spawn(A, S, K_FIB, epaq ? ((n - 1) < cutoff ? 1 : 0) : 0, &cc, nullptr, false, false);
+                c2 = rt_spawn(A, S, K_FIB, epaq ? ((n - 2) < cutoff ? 1 : 0) : 0, &cc, nullptr, false, false);
+            }
             *reinterpret_cast<int4*>(c1) = make_int4(n - 1, 0, 0, 4);
-            FibFrame* c2 = reinterpret_cast<FibFrame*>(
-                rt_spawn(A, S, K_FIB, epaq ? ((n - 2) < cutoff ? 1 : 0) : 0, &cc, nullptr, false, false));
             *reinterpret_cast<int4*>(c2) = make_int4(n - 2, 0, 0, 8);
             // the continuation below (return a + b) is the kJoinSumBit one: the
             // child that completes the join may run it in place of resuming
@@ -965,7 +973,7 @@ struct BuiltinProgramT {
         (void)tid;
         (void)fn;
         switch (kind) {
-            case prog::K_FIB: prog::fib_task(A, S, frame, w0); break;
+            case prog::K_FIB: prog::fib_task<!kSorts && !kGraphs>(A, S, frame, w0); break;
             case prog::K_NQ: prog::nq_task(A, S, frame, w0); break;
             case prog::K_CILKSORT:
                 if (kSorts) prog::cilksort_task(A, S, frame, w0, w1);

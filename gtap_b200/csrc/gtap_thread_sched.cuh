@@ -363,6 +363,75 @@ __device__ __forceinline__ void* rt_spawn(const Arena& A, WarpShared& S, int kin
     return frame_of(A, id);
 }
 
+// The lanes of `m` (calling together) claim two entries each of the counter
+// *p with one shared-memory atomic, laid out as two calls of warp_agg_inc
+// would lay them out: the first entries of all lanes, then the second ones.
+// Returns this lane's first entry; its second is that + popc(m).
+__device__ __forceinline__ int warp_agg_inc2(int* p, unsigned m) {
+    const unsigned lane = lane_id();
+    const int leader = __ffs(m) - 1;
+    int base = 0;
+    if ((int)lane == leader) base = atomicAdd(p, 2 * __popc(m));
+    base = __shfl_sync(m, base, leader);
+    return base + __popc(m & ((1u << lane) - 1u));
+}
+
+// Two attached children on queue 0 at once (the built-in fib): one claim on
+// the id cache and one on the staging buffer serve both, instead of one each
+// per child.  Same effect as two rt_spawn(kind, 0, ...) calls by the lanes
+// of the call: the same ids and staging entries, both headers written, both
+// children counted for the lane.  When an id cannot be had (the arena is exhausted, an error is
+// recorded), the lanes of the call stage their children one by one.
+__device__ __forceinline__ void rt_spawn_pair(const Arena& A, WarpShared& S, int kind, int* child_count,
+                                              void** frame1, void** frame2) {
+    const unsigned lane = lane_id();
+    const unsigned m = __activemask();
+    const int nm = __popc(m);
+    const int a = warp_agg_inc2(&S.alloc_pos, m);
+    const int id1 = a < S.avail_n ? S.avail[(S.avail_head + a) & (kAvailCap - 1)] : alloc_id_slow(A, S);
+    const int id2 = a + nm < S.avail_n ? S.avail[(S.avail_head + a + nm) & (kAvailCap - 1)] : alloc_id_slow(A, S);
+    const int4 hw = make_int4((int)((unsigned)kind << 16), S.l_tid[lane], 0, S.l_root[lane]);
+    const bool ok1 = id1 < A.total_ids, ok2 = id2 < A.total_ids;
+#ifdef GTAP_DEBUG_IDS
+    if (ok1 && atomicExch(&A.dbg_live[id1], 1) != 0) GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, id1, 0, 1, S.l_tid[lane]);
+    if (ok1) atomicExch(&A.dbg_exec[id1], 0);
+    if (ok2 && atomicExch(&A.dbg_live[id2], 1) != 0) GTAP_ERROR(A, ERR_POOL_SLOT_BUSY, id2, 0, 1, S.l_tid[lane]);
+    if (ok2) atomicExch(&A.dbg_exec[id2], 0);
+#endif
+    if (ok1) *reinterpret_cast<int4*>(hdr_of(A, id1)) = hw;
+    if (ok2) *reinterpret_cast<int4*>(hdr_of(A, id2)) = hw;
+    const int tag = (int)(lane << kIdBits);
+    if (__all_sync(m, ok1 && ok2)) {
+        const int s = warp_agg_inc2(&S.cnt[0], m);
+        if (s < A.spawn_cap) S.sbuf[s] = id1 | tag;
+        if (s + nm < A.spawn_cap) S.sbuf[s + nm] = id2 | tag;
+        if (s + nm >= A.spawn_cap) GTAP_ERROR(A, ERR_SPAWN_BUFFER_OVERFLOW, S.l_tid[lane], 0, s + nm, A.spawn_cap);
+        S.l_created[lane] += 2;
+    } else {
+        // a failed allocation takes no staging entry (as in rt_spawn)
+        int made = 0;
+        const unsigned m1 = __ballot_sync(m, ok1);
+        if (ok1) {
+            const int s = warp_agg_inc(&S.cnt[0], m1);
+            if (s < A.spawn_cap) S.sbuf[s] = id1 | tag;
+            else GTAP_ERROR(A, ERR_SPAWN_BUFFER_OVERFLOW, S.l_tid[lane], 0, s, A.spawn_cap);
+            ++made;
+        }
+        const unsigned m2 = __ballot_sync(m, ok2);
+        if (ok2) {
+            const int s = warp_agg_inc(&S.cnt[0], m2);
+            if (s < A.spawn_cap) S.sbuf[s] = id2 | tag;
+            else GTAP_ERROR(A, ERR_SPAWN_BUFFER_OVERFLOW, S.l_tid[lane], 0, s, A.spawn_cap);
+            ++made;
+        }
+        S.l_created[lane] += made;
+    }
+    if (child_count) *child_count += 2;
+    S.l_spawned[lane] += 2;
+    *frame1 = frame_of(A, ok1 ? id1 : A.total_ids);
+    *frame2 = frame_of(A, ok2 ? id2 : A.total_ids);
+}
+
 // taskwait: returns true if the task must suspend (children outstanding).
 // then_sum: the task's code after this taskwait is the kJoinSumBit
 // continuation, which the child completing the join runs in place.
@@ -1329,7 +1398,7 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
         if (one_root) {
             // every task of the round belongs to one root: warp sums, lane 0 books them
             const unsigned value = active ? (unsigned)S.l_value[lane] : 0u;
-            const int w_sum = Prog::kJoinSum ? (int)__reduce_add_sync(0xffffffffu, (unsigned)walked) : 0;
+            const int w_sum = (Prog::kJoinSum && A.join_walk > 0) ? (int)__reduce_add_sync(0xffffffffu, (unsigned)walked) : 0;
             const int f_sum = __popc(fin) + w_sum;
             const int v_sum = (int)__reduce_add_sync(0xffffffffu, value);
             if (lane == 0) {
@@ -1345,7 +1414,7 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
             int f_sum = 0, v_sum = 0;
             if (active) {
                 f_sum = __popc(fin & grp);
-                if (Prog::kJoinSum) f_sum += (int)__reduce_add_sync(grp, (unsigned)walked);
+                if (Prog::kJoinSum && A.join_walk > 0) f_sum += (int)__reduce_add_sync(grp, (unsigned)walked);
                 v_sum = (int)__reduce_add_sync(grp, (unsigned)value);
             }
             const bool leader = active && ((unsigned)__ffs(grp) - 1u == lane);
@@ -1373,7 +1442,7 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
         const unsigned created_all = __reduce_add_sync(0xffffffffu, (unsigned)(active ? S.l_created[lane] : 0));
         if (lane == 0) S.st[GTAP_STAT_TASKS] += created_all;
 #ifndef GTAP_PHASE_TIMERS
-        if (Prog::kJoinSum) {
+        if (Prog::kJoinSum && A.join_walk > 0) {
             const unsigned walked_all = __reduce_add_sync(0xffffffffu, (unsigned)walked);
             if (lane == 0) S.st[GTAP_STAT_JOIN_FINISHES] += walked_all;
         }
