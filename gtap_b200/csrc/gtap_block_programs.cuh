@@ -259,12 +259,12 @@ __device__ void mergesort_task(const Arena& A, BlockShared& S, int* smem) {
 
 // gtap_fib.cu:10-22 with fib_queue_1.cu's sequential cutoff; one block per task.
 __device__ void fib_task(const Arena& A, BlockShared& S) {
-    const int4 fr = S.w0;   // {n, a, b, slot}
+    const int4 fr = S.w0;   // {n, a, b, slot}: the root's frame also carries thread mode's settings above the slot byte
     int st = bt_state(S);
     if (st == 0) {
         const int n = fr.x, cutoff = bt_root(A, S).i1;
         if (n < 2 || n < cutoff) {
-            if (threadIdx.x == 0) bt_return_i32(A, S, fr.w, n < 2 ? n : prog::fib_sequential(n));
+            if (threadIdx.x == 0) bt_return_i32(A, S, fr.w & prog::kFibSlotMask, n < 2 ? n : prog::fib_sequential(n));
             bt_finish(S);
             return;
         }
@@ -276,7 +276,7 @@ __device__ void fib_task(const Arena& A, BlockShared& S) {
         st = 1;
     }
     if (st == 1) {
-        if (threadIdx.x == 0) bt_return_i32(A, S, fr.w, fr.y + fr.z);
+        if (threadIdx.x == 0) bt_return_i32(A, S, fr.w & prog::kFibSlotMask, fr.y + fr.z);
     } else if (threadIdx.x == 0) {
         GTAP_ERROR(A, ERR_INVALID_TASKWAIT, S.task, -1, st, 1);
     }

@@ -264,8 +264,9 @@ constexpr uint8_t kFlagJoinFinish = 0x10;   // block mode: after its taskwait th
 constexpr uint8_t kKindIndirect = 255;
 constexpr int kJoinCountMask = 0x00FFFFFF;
 // Thread mode: the task's code after its taskwait returns frame word 1 + frame
-// word 2 (int32, wrapping) into its parent's frame at the byte offset in frame
-// word 3 (into the root's result for a root task) and finishes.  The child
+// word 2 (int32, wrapping) into its parent's frame at the byte offset in the
+// low byte of frame word 3 (into the root's result for a root task) and
+// finishes.  The child
 // whose join decrement sees this bit with a count of one does exactly that in
 // place of resuming the task, and goes on to the grandparent's join.
 constexpr int kJoinSumBit = 1 << 27;

@@ -57,8 +57,11 @@ struct FibFrame {
     int n;
     int a;     // result of fib(n-1), written by child 1
     int b;     // result of fib(n-2), written by child 2
-    int slot;  // byte offset of this task's result in its parent's frame
+    int slot;  // bits 0-7: byte offset of this task's result in its parent's frame; the root's settings,
+               // copied to every task so none reads the root descriptor: bits 8-15 the serial cutoff
+               // (clamped to 0..65, n <= 64), bit 16 the EPAQ variant (root.i2 != 0 and 3+ queues)
 };
+constexpr int kFibSlotMask = 0xFF;
 
 // fib_queue_1.cu:9-14: visits the same call tree as the reference's doubly
 // recursive fib_sequential (every node n >= 2 expands into n-1 and n-2, every
@@ -94,19 +97,18 @@ __device__ __forceinline__ void fib_task(const Arena& A, WarpShared& S, void* fr
     int4 fr = w0;   // {n, a, b, slot}, loaded with the header
     switch (rt_state(S)) {
         case 0: {
-            const gtap_root& rd = root_of(A, S);
-            const int n = fr.x, cutoff = rd.i1;
+            const int n = fr.x, cutoff = (fr.w >> 8) & 0xFF;
             if (n < 2) {
-                return_i32(A, S, fr.w, n);
+                return_i32(A, S, fr.w & kFibSlotMask, n);
                 rt_finish(S);
                 return;
             }
             if (n < cutoff) {
-                return_i32(A, S, fr.w, fib_sequential(n));
+                return_i32(A, S, fr.w & kFibSlotMask, fib_sequential(n));
                 rt_finish(S);
                 return;
             }
-            const bool epaq = rd.i2 != 0 && A.num_queues >= 3;
+            const bool epaq = (fr.w >> 16) & 1;
             int cc = 0;
             void* c1;
             void* c2;
@@ -116,8 +118,9 @@ __device__ __forceinline__ void fib_task(const Arena& A, WarpShared& S, void* fr
                 c1 = rt_spawn(A, S, K_FIB, epaq ? ((n - 1) < cutoff ? 1 : 0) : 0, &cc, nullptr, false, false);
                 c2 = rt_spawn(A, S, K_FIB, epaq ? ((n - 2) < cutoff ? 1 : 0) : 0, &cc, nullptr, false, false);
             }
-            *reinterpret_cast<int4*>(c1) = make_int4(n - 1, 0, 0, 4);
-            *reinterpret_cast<int4*>(c2) = make_int4(n - 2, 0, 0, 8);
+            const int settings = fr.w & ~kFibSlotMask;
+            *reinterpret_cast<int4*>(c1) = make_int4(n - 1, 0, 0, settings | 4);
+            *reinterpret_cast<int4*>(c2) = make_int4(n - 2, 0, 0, settings | 8);
             // the continuation below (return a + b) is the kJoinSumBit one: the
             // child that completes the join may run it in place of resuming
             // this task (gtap_config::join_walk)
@@ -126,7 +129,7 @@ __device__ __forceinline__ void fib_task(const Arena& A, WarpShared& S, void* fr
         }
         // fallthrough
         case 1: {
-            return_i32(A, S, fr.w, fr.y + fr.z);
+            return_i32(A, S, fr.w & kFibSlotMask, fr.y + fr.z);
             rt_finish(S);
             return;
         }
@@ -846,9 +849,12 @@ struct BuiltinProgramT {
         (void)A;
         int4* f = reinterpret_cast<int4*>(frame);
         switch (rd.kind) {
-            case GTAP_KIND_FIB:
-                f[0] = make_int4(rd.i0, 0, 0, 0);
+            case GTAP_KIND_FIB: {
+                const int cutoff = rd.i1 < 0 ? 0 : (rd.i1 > 65 ? 65 : rd.i1);
+                const int epaq = (rd.i2 != 0 && A.num_queues >= 3) ? 1 : 0;
+                f[0] = make_int4(rd.i0, 0, 0, cutoff << 8 | epaq << 16);   // slot 0: the root's result
                 break;
+            }
             case GTAP_KIND_NQ:
                 f[0] = make_int4(0 | (rd.i0 << 8) | (rd.i1 << 16), 0, 0, 0);
                 break;

@@ -504,7 +504,7 @@ static __device__ __noinline__ int join_sum_walk(const Arena& A, WarpShared& S, 
         const int4 f = ld_cg_v4(frame_of(A, p));
         const int gp = h.y;
         const int v = (int)((unsigned)f.y + (unsigned)f.z);
-        if (gp >= 0) *reinterpret_cast<int*>(reinterpret_cast<char*>(frame_of(A, gp)) + f.w) = v;
+        if (gp >= 0) *reinterpret_cast<int*>(reinterpret_cast<char*>(frame_of(A, gp)) + (f.w & 0xFF)) = v;
         else A.results[h.w].value = v;
         rt_release_id_dbg(A, p);
         if (!(((unsigned)h.x >> 24) & kFlagRetain)) rt_release_id(A, S, p);
