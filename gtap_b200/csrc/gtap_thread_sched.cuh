@@ -147,6 +147,13 @@ __device__ __forceinline__ void qset(T (&a)[N], int k, typename QNoDeduce<T>::ty
         if (k == i) a[i] = v;
 }
 
+// The queues a kernel serves: a kernel built for one queue (QM == 1) only
+// runs launches with one, so the count folds to a constant there.
+template <int QM>
+__device__ __forceinline__ int queue_count(const Arena& A) {
+    return QM == 1 ? 1 : A.num_queues;
+}
+
 template <int QM>
 __device__ __forceinline__ void queue_pos_init(QueuePos<QM>& P) {
 #pragma unroll
@@ -821,7 +828,7 @@ static __device__ void publish_commit(const Arena& A, WarpShared& S, QueuePos<QM
     __syncwarp();   // every lane's fence is done before lane 0 publishes
     if (any) {
         if (lane == 0) {
-            for (int k = 0; k < A.num_queues; ++k) {
+            for (int k = 0; k < queue_count<QM>(A); ++k) {
                 const int d = qget(P.pend, k);
                 if (d) {
                     red_add_relaxed(dq_ctl_ptr(A, k, S.worker), (unsigned long long)d << kPosBits);
@@ -1002,7 +1009,7 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
         if (nb == 0) {
             // acquire: own deque, then steal, per EPAQ queue starting at cur_q
             // (reference :896-926), then the overflow queue, then new roots.
-            const int Q = A.num_queues;
+            const int Q = queue_count<QM>(A);
             for (int kk = 0; kk < Q && nb == 0; ++kk) {
                 int k = (P.cur_q + kk) % Q;
                 nb = pop_own(A, S, P, k, my_tid);
@@ -1149,7 +1156,7 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
             const int have = S.cnt[0];
             const bool orphans = __any_sync(0xffffffffu, (int)lane < nb && (S.l_flags[lane] & kLaneFinished) &&
                                                              S.l_spawned[lane] > 0);
-            if (A.num_queues != 1 || have <= 0 || have > A.spawn_cap || orphans) break;
+            if (queue_count<QM>(A) != 1 || have <= 0 || have > A.spawn_cap || orphans) break;
             const int k = min(have, kWarp - nb);
             // lane nb + j takes the j-th newest staged child; the staging
             // entries were written (and the children's records and frames)
@@ -1230,7 +1237,7 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
         }
         // (1) orphans: children of tasks that returned without a taskwait
         if (fin & spawners) {
-            for (int q = 0; q < A.num_queues; ++q) {
+            for (int q = 0; q < queue_count<QM>(A); ++q) {
                 const int n = min(S.cnt[q], A.spawn_cap);
                 const int* sb = S.sbuf + q * A.spawn_cap;
                 for (int e = (int)lane; e < n; e += 32) {
@@ -1269,7 +1276,7 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
                         resumed = join_sum_walk(A, S, parent, walked, rq);
                     } else {
                         rq = (old >> 24) & 7;
-                        if (rq >= A.num_queues) rq = 0;
+                        if (rq >= queue_count<QM>(A)) rq = 0;
                         resumed = parent;
                     }
                 }
@@ -1290,7 +1297,7 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
         //     hungry (always, with eager publication), and published in (5).
         int kn = -1;
         {
-            const int Q = A.num_queues;
+            const int Q = queue_count<QM>(A);
             // eager publication behaves as if some worker were always hungry
             const int hungry = A.publish_lazy ? __shfl_sync(0xffffffffu, hv, 0) : 1;
             const int reserve = A.publish_lazy ? kReserve : 0;
@@ -1435,7 +1442,7 @@ static __device__ void worker_loop(const Arena& A, WarpShared& S, int initial_ti
         }
         __syncwarp();
         if (lane == 0) {
-            for (int k = 0; k < A.num_queues; ++k) S.cnt[k] = 0;
+            for (int k = 0; k < queue_count<QM>(A); ++k) S.cnt[k] = 0;
             S.st[GTAP_STAT_EXECUTIONS] += (unsigned long long)nb;
             S.st[GTAP_STAT_ROUNDS] += 1;
         }
