@@ -434,9 +434,29 @@ static __device__ __noinline__ void warp_sort(const int* in, int* out, int* scr,
     __syncwarp();
 }
 
-// cilksort.cu:38-49: largest index with x[idx] <= val
-__device__ __forceinline__ int bsearch_le(const int* x, int len, int val) {
+// cilksort.cu:38-49: largest index with x[idx] <= val.  The answer is the
+// binary search's.  quad: three probes per step, loaded together, keep a
+// quarter of the interval, so a split costs half the dependent loads (10 steps
+// instead of 20 for 2^20 keys) for 1.5x the loads and more instructions.
+// Invariant: x[low] <= val (or low == -1) and x[high] > val (or high == len).
+__device__ __forceinline__ int bsearch_le(const int* x, int len, int val, bool quad) {
     int low = -1, high = len;
+    while (quad && high - low > 4) {
+        const int q = (high - low) / 4;
+        const int m1 = low + q, m2 = low + 2 * q, m3 = low + 3 * q;   // low < m1 < m2 < m3 < high
+        const int v1 = ld_data(x + m1), v2 = ld_data(x + m2), v3 = ld_data(x + m3);
+        if (v3 <= val) {
+            low = m3;
+        } else if (v2 <= val) {
+            low = m2;
+            high = m3;
+        } else if (v1 <= val) {
+            low = m1;
+            high = m2;
+        } else {
+            high = m1;
+        }
+    }
     while (low + 1 < high) {
         int mid = (low + high) / 2;
         if (ld_data(x + mid) <= val) low = mid;
@@ -472,14 +492,20 @@ __device__ __forceinline__ void cilkmerge_task(const Arena& A, WarpShared& S, vo
         const int* t = a; a = b; b = t;
         int tl = alen; alen = blen; blen = tl;
     }
-    const int cutoff = root_of(A, S).i1;
+    const gtap_root& rd = root_of(A, S);
+    const int cutoff = rd.i1;
     if (blen == 0 || alen + blen < cutoff) {   // a copy or a leaf merge: warp_leaves does it
         mark_leaf(S);
         rt_finish(S);
         return;
     }
     const int as = (alen + 1) / 2;
-    const int bs = bsearch_le(b, blen, ld_data(a + as - 1)) + 1;
+    // Sorts of 2^22 keys or more search their splits four ways: their depth of
+    // dependent splits sets their time (mergesort of 2^24 keys 6.27 -> 5.85 ms,
+    // cilksort of 10^7..10^8 keys 2-5 % faster).  Smaller sorts, such as the
+    // mix's (at most 2^20 keys), run many short searches at once, where the
+    // extra loads and instructions cost more (its sort launch 22.5 -> 22.8 ms).
+    const int bs = bsearch_le(b, blen, ld_data(a + as - 1), rd.n >= (1ll << 22)) + 1;
     int cc = 0;
     spawn_merge(A, S, &cc, a, as, b, bs, dst);
     spawn_merge(A, S, &cc, a + as, alen - as, b + bs, blen - bs, dst + as + bs);
