@@ -82,6 +82,10 @@ def test_invalid_config_rejected():
     assert gt.lib().gtap_initialize(ctypes.byref(c)) == gt.ERROR_INVALID_ARGUMENT
     c = gt.default_config(num_queues=5)
     assert gt.lib().gtap_initialize(ctypes.byref(c)) == gt.ERROR_INVALID_ARGUMENT
+    # rounds that walk fib's sums at their joins: 0..32 tasks; extra passes on idle lanes: 0..8
+    for field, bad in (("join_walk", -1), ("join_walk", 33), ("sub_rounds", -1), ("sub_rounds", 9)):
+        c = gt.default_config(**{field: bad})
+        assert gt.lib().gtap_initialize(ctypes.byref(c)) == gt.ERROR_INVALID_ARGUMENT, (field, bad)
 
 
 def test_gen_keys_matches_oracle_and_std():
